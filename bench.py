@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""MLEM throughput on one B200 (or N, views sharded) -- one JSON line on rank 0.
+
+Workload: 256^3 FP32 volume of 0.25 mm voxels, 360 views of a 512x512
+detector of 0.5 mm pixels (source-isocentre 500 mm, source-detector 800 mm),
+seeded 40-ellipsoid phantom, Poisson noise at I0 = 1e5.  A step is one MLEM
+iteration: forward projection of all 360 views with the ratio g / Hf fused
+in, then back projection of the ratios with the update f <- f*Ht/sens fused
+in.  Inputs (the 377 MB measured sinogram and the ratio sinogram) are larger
+than the L2 cache, so no flush is inserted between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl recon_b200|reference]
+
+--impl reference times the reference's own CPU path: its Siddon kernel
+sources compiled for the host (oracle/_ref/libref_cpu.so), run with its
+step-synchronous per-view structure on all host threads, on a bounded sample
+of views of one MLEM iteration, extrapolated to iterations per second.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLEM iters/s & ray-voxel isects/s, batched vs plain on 1 B200 at <=1e-4 rel L2 vs FP64"
+UNIT = "MLEM iter/s"
+WORKLOAD = "plain_gpu_256cube_360x512x512"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="recon_b200", choices=["recon_b200", "reference"])
+    ap.add_argument("--sum", default="kahan", choices=["kahan", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-baseline-views", type=int, default=1)
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index: int):
+        self.lines: list[str] = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index), "--query-gpu=" + ",".join(self.FIELDS),
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids) and ids[local_rank].strip().isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+def make_problem(cfg, device):
+    """Phantom and noisy measurement for the workload, built on the device."""
+    import torch
+
+    from recon_b200 import Plan
+    from recon_b200.phantom import noisy, phantom
+
+    vol = torch.from_numpy(phantom(cfg)).to(device)
+    P0 = Plan(cfg)
+    p = P0.fp_views(vol)
+    g = noisy(p, cfg["I0"], cfg["seed"])
+    del p
+    return vol, g
+
+
+def cpu_baseline(cfg, g_host, nviews: int):
+    """The reference's kernels built for the host, single thread, on a sample of
+    views of the first MLEM iteration (f = 1), extrapolated to iterations/s."""
+    import numpy as np
+
+    from oracle import oracle as O
+    from recon_b200.configs import geom_dict
+
+    R = O.ref_cpu()
+    if R is None:
+        return None
+    R.ref_cpu_set_threads(1)
+    geo = O.Geom.from_dict(geom_dict(cfg))
+    f = np.ones(geo.nvox, np.float32)
+    ht = np.zeros(geo.nvox, np.float32)
+    n = int(cfg["NumProj"])
+    views = [int(round(k * n / nviews)) % n for k in range(nviews)]
+    t0 = time.perf_counter()
+    for v in views:
+        ang = float(np.float32(v) * np.float32(cfg["DeltaAng"]))
+        loopN = O.c_loopN(geo, ang)
+        R.ref_cpu_mlem_view(geo, ang, loopN, f, np.ascontiguousarray(g_host[v].ravel()), ht)
+    dt = (time.perf_counter() - t0) / len(views)
+    return {"value": 1.0 / (dt * n), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{len(views)} of {n} views of one MLEM iteration (FP + ratio + BP, the reference's "
+                      f"step-synchronous kernels built for the host), {dt:.2f} s/view, extrapolated x{n}"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import numpy as np
+
+    from recon_b200.configs import PLAIN_GPU, geom_dict
+
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True}
+    try:
+        from oracle import oracle as O
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({**base, "unavailable": f"checker package not importable: {e}"}))
+        return
+    R = O.ref_cpu()
+    if R is None:
+        print(json.dumps({**base, "unavailable": "reference host build oracle/_ref/libref_cpu.so missing"}))
+        return
+    cfg = dict(PLAIN_GPU)
+    threads = os.cpu_count() or 1
+    R.ref_cpu_set_threads(threads)
+    geo = O.Geom.from_dict(geom_dict(cfg))
+    from recon_b200.phantom import noisy, phantom
+
+    vol = phantom(cfg).astype(np.float64).ravel()
+    n = int(cfg["NumProj"])
+    dang = np.float32(cfg["DeltaAng"])
+    nsample = max(1, args.steps + args.warmup)
+    views = [int(round(k * n / nsample)) % n for k in range(nsample)]
+    gviews = {}
+    for v in sorted(set(views)):
+        img = np.zeros(geo.npix)
+        O.lib().orc_x_fp_view(geo, float(np.float32(v) * dang), vol, img)
+        gviews[v] = noisy(img, cfg["I0"], cfg["seed"] + v).astype(np.float32)
+    f = np.ones(geo.nvox, np.float32)
+    ht = np.zeros(geo.nvox, np.float32)
+    times = []
+    for k, v in enumerate(views):
+        ang = float(np.float32(v) * dang)
+        loopN = O.c_loopN(geo, ang)
+        t0 = time.perf_counter()
+        R.ref_cpu_mlem_view(geo, ang, loopN, f, gviews[v], ht)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+    tv = sum(times) / len(times)
+    value = 1.0 / (tv * n)
+    sample = (f"{len(times)} timed views (+{args.warmup} warm-up) of one MLEM iteration of the 256^3 / 360-view "
+              f"workload with the reference's step-synchronous kernels built for the host, {tv:.3f} s/view on "
+              f"{threads} threads, extrapolated x{n}")
+    print(json.dumps({
+        **base, "value": value, "n_gpus": world, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": tv * n * 1e3, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 40-ellipsoid phantom, Poisson I0=1e5)",
+        "config": {"workload": WORKLOAD, "volume": [256, 256, 256], "views": n, "detector": [512, 512]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from recon_b200 import SUM_KAHAN, SUM_PLAIN, Options, Plan
+    from recon_b200.configs import PLAIN_GPU
+    from recon_b200.sharding import ordered_sum_, view_range
+
+    world, rank, local = dist_env()
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    cfg = dict(PLAIN_GPU)
+    opts = Options(sum=SUM_KAHAN if args.sum == "kahan" else SUM_PLAIN, device=local)
+    vol, g = make_problem(cfg, device)
+    P = Plan(cfg, opts)
+    nviews = int(cfg["NumProj"])
+    isects = P.count_intersections()
+    P.mlem_prepare()
+    f = P.new_volume(1.0)
+    ht = P.new_volume(0.0)
+    first, count = view_range(nviews, rank, world)
+    npix = P.nu * P.nv
+    nvox = f.numel()
+
+    def iteration(ev=None):
+        if world == 1:
+            if ev:
+                ev[0].record()
+            P.mlem_forward(g, f)
+            if ev:
+                ev[1].record()
+            P.mlem_backward_update(f)
+            if ev:
+                ev[2].record()
+        else:
+            P.mlem_forward(g, f, first, count)
+            P.mlem_backward(ht, first, count)
+            ordered_sum_(ht)
+            P.mlem_update(f, ht)
+
+    for _ in range(args.warmup):
+        iteration()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(gpu_index(local)) if rank == 0 else None
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for k in range(args.steps):
+        iteration(evs[k] if world == 1 else None)
+    end.record()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    ms_step = ms / args.steps
+    value = 1e3 / ms_step
+
+    # end to end through the C ABI with host buffers: upload the measured
+    # sinogram from pinned memory, iterate, read the image back, every step
+    g_host = g.cpu().pin_memory() if world == 1 else None
+    f_host = torch.empty(f.shape, dtype=torch.float32).pin_memory() if world == 1 else None
+    e2e = None
+    if world == 1:
+        gdev = torch.empty_like(g)
+        for _ in range(max(1, args.warmup)):
+            gdev.copy_(g_host, non_blocking=True)
+            P.mlem_iteration(gdev, f)
+            f_host.copy_(f, non_blocking=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            gdev.copy_(g_host, non_blocking=True)
+            P.mlem_iteration(gdev, f)
+            f_host.copy_(f, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        e2e_ms = a.elapsed_time(b) / args.steps
+        e2e = {"value": 1e3 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": g.numel() * g.element_size(),
+               "d2h_bytes_per_step": f.numel() * 4}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 40-ellipsoid phantom in a 0.02/mm cylinder, Poisson noise I0=1e5)",
+        "config": {"workload": WORKLOAD, "volume": [256, 256, 256], "voxel_mm": 0.25, "views": nviews,
+                   "detector": [512, 512], "pixel_mm": 0.5, "arith": "exact",
+                   "sum": args.sum, "parallelism": f"views/{world}" if world > 1 else "single",
+                   "l2": "no flush: per-step inputs (377 MB sinogram + 377 MB ratio) exceed the 126 MB L2"},
+        "isects_per_pass": isects,
+        "isects_per_s": 2.0 * isects * value,
+        "gpu_launches": 2 * args.steps if world == 1 else 3 * args.steps,
+    }
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    if world == 1:
+        t_fp = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
+        t_bp = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
+        bytes_fp = 4.0 * isects + 4.0 * npix * nviews
+        bytes_bp = 4.0 * isects + 12.0 * nvox
+        dom = ("bp_gather", t_bp, bytes_bp) if t_bp >= t_fp else ("fp_ratio", t_fp, bytes_fp)
+        ach = dom[2] / (dom[1] * 1e-3) / 1e9
+        out["roofline"] = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": hbm, "unit": "GB/s",
+                           "frac": ach / hbm, "peak_source": peak_src, "traffic": None,
+                           "algorithmic_bytes_per_launch": dom[2], "launch_ms": dom[1]}
+        b_iter = 8.0 * isects + 4.0 * npix * nviews + 12.0 * nvox
+        out["iteration_roofline"] = {"bytes_per_iteration": b_iter, "achieved_gbs": b_iter / (ms_step * 1e-3) / 1e9,
+                                     "frac": b_iter / (ms_step * 1e-3) / 1e9 / hbm,
+                                     "fp_ms": t_fp, "bp_ms": t_bp}
+    out["e2e"] = e2e
+    out["clocks"] = clk
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(cfg, g_host.numpy().reshape(nviews, P.nv, P.nu),
+                                               args.cpu_baseline_views)
+        except Exception as e:  # pragma: no cover
+            out["cpu_baseline"] = {"error": str(e)}
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,15 @@
+"""B200-native MLEM cone-beam reconstruction on a Siddon projector pair.
+
+The compute lives in ``librecon_b200.so`` (hand-written sm_100a CUDA behind the
+C ABI of ``include/recon_b200.h``); this package is its Python face.
+"""
+from ._lib import (ARITH_COMPAT, ARITH_EXACT, BP_SIDDON, BP_VOXEL, SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN,
+                   VOXEL_GEOMETRIC, VOXEL_REFERENCE, ReconError)
+from .api import (Options, Plan, backward_projection_from_cfg, forward_projection_from_cfg, geometry,
+                  geometry_from_cfg, mlem_from_cfg)
+
+__all__ = [
+    "ARITH_COMPAT", "ARITH_EXACT", "BP_SIDDON", "BP_VOXEL", "SINO_BF16", "SINO_F32", "SUM_KAHAN", "SUM_PLAIN",
+    "VOXEL_GEOMETRIC", "VOXEL_REFERENCE", "ReconError", "Options", "Plan", "geometry", "geometry_from_cfg",
+    "mlem_from_cfg", "forward_projection_from_cfg", "backward_projection_from_cfg",
+]

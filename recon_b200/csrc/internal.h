@@ -1,0 +1,179 @@
+// internal.h -- shared declarations of librecon_b200 (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/recon_b200.h"
+
+namespace rb {
+
+// ---- error plumbing -------------------------------------------------------
+
+void set_error(const std::string& msg);
+recon_status_t fail(recon_status_t code, const std::string& msg);
+recon_status_t cuda_fail(cudaError_t e, const char* what);
+
+#define RB_CUDA(call)                                            \
+    do {                                                         \
+        cudaError_t rb_e_ = (call);                              \
+        if (rb_e_ != cudaSuccess) return ::rb::cuda_fail(rb_e_, #call); \
+    } while (0)
+#define RB_CHECK(call)                                   \
+    do {                                                 \
+        recon_status_t rb_s_ = (call);                   \
+        if (rb_s_ != RECON_OK) return rb_s_;             \
+    } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---- geometry passed to kernels by value ----------------------------------
+
+// COMPAT arithmetic: the reference's XraySystem (siddon_device_kernelsMLEM.cuh:27-48)
+// flattened, plus the 3x3 detector rotation.
+struct CompatGeom {
+    float R, Rf, Ry, Dx, Dz, M;
+    float NumAxPixels_f, NumTAxPixels_f, AxPixDimMm, TAxPixDimMm;
+    float Pi[3], Pf[3], Pd[3], Xs[3];
+    float RM[9];
+    int dims[3];
+    int Nu, Nv;
+};
+
+// EXACT arithmetic: plane crossings along a ray are parameterised by
+// t = R*alpha - Rf, the depth along the view's central axis in mm (alpha is
+// the ray parameter from source (0) to detector pixel (1)).  Plane k of an
+// axis sits at t(k) = fmaf(float(k - kc), S, O), with S, O, kc set up in FP64
+// per ray so that |t| is small where planes cross the volume.  The segment
+// length in mm is (t1 - t0) * w with w = |p2 - p1| / R.
+struct AxisT {
+    float S, O;
+    int kc;
+};
+struct ZParam {  // per detector row v (z planes)
+    float S, O, inv_S;
+    int kc;
+};
+struct ExactGeom {
+    int X, Y, Z;        // voxels
+    int Nu, Nv;         // detector columns (u) / rows (v)
+    float vox[3];       // voxel size per axis
+    float P0[3];        // first plane per axis (-dim/2*vox)
+    float R, Rf, Ry, Dx, Dz;
+    float ud0, du;      // detector u coordinate of pixel 0 and pitch (mm, before R/Ry)
+    float vd0, dv;
+};
+
+// ---- plan -------------------------------------------------------------------
+
+struct DeviceBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Plan {
+    recon_geometry_t geom{};
+    recon_options_t opt{};
+    int device = 0;
+    int sm_count = 148;
+    size_t npix = 0, nvox = 0;
+    unsigned nviews = 0;
+    std::vector<float> view_angles;  // (float)n * DeltaAng
+    float RM[9];
+
+    CompatGeom cg{};
+    ExactGeom eg{};
+
+    // EXACT tables (device)
+    float4* d_txy = nullptr;   // [view][u] {Sx, Ox, Sy, Oy}
+    int2* d_kxy = nullptr;     // [view][u] {kcx, kcy}
+    float2* d_cs = nullptr;    // [view] {cos, sin} of the view angle
+    ZParam* d_zp = nullptr;    // [v]
+    float* d_w = nullptr;      // [v][u] |p2-p1| / R
+    // scratch view slot for arbitrary-angle single-view calls (index nviews)
+    float* d_angles = nullptr;    // [view] (float)n*DeltaAng, + 1 scratch slot
+    // COMPAT tables
+    unsigned* d_loopN = nullptr;  // [view] (+1 scratch slot)
+    // workspaces
+    float* d_sens = nullptr;      // cached sensitivity
+    bool sens_valid = false;
+    void* d_ratio = nullptr;      // ratio sinogram (float or bf16) [nviews][npix]
+    float* d_ht = nullptr;        // COMPAT: Ht accumulator [nvox]
+    unsigned long long* d_fix = nullptr;  // COMPAT: fixed-point accumulator [nvox]
+    unsigned* d_maxabs = nullptr; // COMPAT: per-view max |value| bits [nviews+1]
+    float* d_view_img = nullptr;  // scratch image [npix]
+    size_t device_bytes = 0;
+    std::vector<void*> allocations;
+
+    template <class T>
+    recon_status_t alloc(T** p, size_t count, const char* what);
+    ~Plan();
+};
+
+template <class T>
+recon_status_t Plan::alloc(T** p, size_t count, const char* what)
+{
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? RECON_ERR_OUT_OF_MEMORY : RECON_ERR_CUDA,
+                    std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
+    }
+    allocations.push_back(q);
+    device_bytes += count * sizeof(T);
+    *p = static_cast<T*>(q);
+    return RECON_OK;
+}
+
+// ---- entry points implemented in the .cu files --------------------------------
+
+recon_status_t build_compat_tables(Plan& P, cudaStream_t s);
+recon_status_t build_exact_tables(Plan& P, cudaStream_t s);
+recon_status_t exact_view_table(Plan& P, float angle, cudaStream_t s);  // into slot nviews
+recon_status_t compat_view_loopN(Plan& P, float angle, unsigned slot, cudaStream_t s);
+
+// FP: views [first, first+count) (angles from the plan) or the scratch slot.
+// mode 0: write projections; mode 1: MLEM ratio (g/Hf, times w for EXACT)
+recon_status_t exact_fp(Plan& P, const float* vol, unsigned first, unsigned count, bool scratch_slot,
+                        float* out, cudaStream_t s);
+recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ratio, cudaStream_t s,
+                              unsigned first, unsigned count);
+recon_status_t exact_count(Plan& P, unsigned long long* out);
+// BP gather over views [first, first+count) of `sino` (weighted by w) into vol (overwrite);
+// sens_mode: back project ones; update: f = f*Ht/sens in the epilogue.
+recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, unsigned first,
+                        unsigned count, bool scratch_slot, bool sens_mode, float* vol,
+                        const float* sens, float* f_update, cudaStream_t s);
+
+recon_status_t compat_fp(Plan& P, const float* vol, unsigned first, unsigned count, bool scratch_slot,
+                         float angle_scratch, float* out, cudaStream_t s);
+recon_status_t compat_bp_view(Plan& P, const float* img, unsigned view, bool scratch_slot,
+                              float angle_scratch, float* out_or_accum, bool accumulate,
+                              cudaStream_t s);
+recon_status_t compat_mlem_iteration(Plan& P, const float* g, float* f, cudaStream_t s);
+recon_status_t compat_sensitivity(Plan& P, float* sens, cudaStream_t s);
+
+recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned count, bool scratch_slot,
+                        float angle_scratch, unsigned Nproj, int mode, bool ones, float* vol_accum,
+                        const float* sens, float* f_update, cudaStream_t s);
+recon_status_t plain_fp_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
+recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
+recon_status_t compat_fp_ratio_all(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
+void release_plan_textures(const Plan* P);
+recon_status_t ensure_mlem_buffers(Plan& P);
+recon_status_t compute_sensitivity(Plan& P, float* sens, cudaStream_t s);
+
+recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);
+recon_status_t launch_update(float* f, const float* ht, const float* sens, size_t n, bool fast_div,
+                             cudaStream_t s);
+recon_status_t launch_fill(float* a, float v, size_t n, cudaStream_t s);
+
+}  // namespace rb
+
+// The opaque handle of the C ABI is the plan itself.
+struct recon_plan : rb::Plan {};

@@ -1,0 +1,318 @@
+// voxel.cu -- voxel-driven back projection (the reference's
+// backward_projection / backward_projection2, CT_Recon/hf_cuda_kernels.cuh:
+// 183-284) as a deterministic gather: one thread per voxel, a loop over views
+// inside the thread, the running sum in a register (added in view order, as
+// the reference's per-view launches add into the volume), and the MLEM update
+// f <- f * Ht / sens fused into the epilogue when requested.
+//
+// REFERENCE mode keeps backward_projection2's arithmetic and its flat-array
+// bilinear taps (a tap beyond the image end reads 0).  GEOMETRIC mode uses the
+// Siddon projector's angle sense and pixel units and samples the view image
+// through a texture object (point fetches, FP32 bilinear weights -- hardware
+// linear filtering has 8-bit weights); the reference samples through a legacy
+// texture reference with the Ruijters cubic B-spline library, which is not
+// part of the reference, so that variant cannot be reproduced.
+#include <unordered_map>
+
+#include "internal.h"
+
+namespace rb {
+namespace voxel {
+
+struct VGeom {
+    int X, Y, Z, Nu, Nv;
+    float vox[3];
+    float R, Rf, Ry, Dx, Dz, M, du_mm, dv_mm;  // pitches in mm (not times M)
+    float RM[9];
+};
+
+// pixel_iterate (hf_cuda_kernels.cuh:83-87)
+__device__ __forceinline__ float center(float NumPixels, float PixelsDimMm, float Mag, int iterator)
+{
+    return -(NumPixels - 1.0f) / 2.0f * PixelsDimMm * Mag + (float)iterator * PixelsDimMm * Mag;
+}
+
+template <bool TEX>
+__device__ __forceinline__ float tap(const float* img, cudaTextureObject_t tex, int u, int v, int Nu)
+{
+    if (TEX) return tex2D<float>(tex, (float)u + 0.5f, (float)v + 0.5f);
+    return __ldg(img + (size_t)v * Nu + u);
+}
+
+// MODE 0: vol += sum over views; MODE 1: sensitivity (ones images);
+// MODE 2: MLEM update f = (s != 0) ? f * Ht / s : 0.
+template <int VMODE, int MODE, bool TEX>
+__global__ void __launch_bounds__(128) bp_kernel(VGeom G, const float* __restrict__ angles, unsigned view0,
+                                                  unsigned nview, unsigned Nproj, const float* __restrict__ sino,
+                                                  const cudaTextureObject_t* __restrict__ texs,
+                                                  float* __restrict__ vol, const float* __restrict__ sens)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= G.X || y >= G.Y) return;
+    const size_t n = (size_t)x + (size_t)y * G.X + (size_t)z * G.X * G.Y;
+    const size_t npix = (size_t)G.Nu * G.Nv;
+    const float xo = center((float)G.X, G.vox[0], 1.0f, x);
+    const float yo = center((float)G.Y, G.vox[1], 1.0f, y);
+    const float zo = center((float)G.Z, G.vox[2], 1.0f, z);
+    const float* RM = G.RM;
+    const float R = G.R, Rf = G.Rf, Ry = G.Ry;
+    float acc = (MODE == 0) ? vol[n] : 0.0f;
+    for (unsigned vi = 0; vi < nview; ++vi) {
+        const float alpha = angles[view0 + vi];
+        const float* img = sino + vi * npix;
+        cudaTextureObject_t tex = TEX ? texs[vi] : 0;
+        if (VMODE == RECON_VOXEL_REFERENCE) {
+            // backward_projection2 (hf_cuda_kernels.cuh:240-284), as written
+            const float sin_alpha = sinf(alpha * (float)3.1415927 / 180.0f);
+            const float cos_alpha = cosf(alpha * (float)3.1415927 / 180.0f);
+            const float x_alpha = xo * cos_alpha + yo * sin_alpha;
+            const float y_alpha = -xo * sin_alpha + yo * cos_alpha;
+            const float u_id = __fdividef(R * x_alpha, y_alpha + Rf);
+            const float v_id = __fdividef(R * zo, y_alpha + Rf);
+            const float detQ = (RM[0] - RM[3] * u_id / R) * (RM[8] - RM[5] * v_id / R) -
+                               (RM[2] - RM[5] * u_id / R) * (RM[6] - RM[3] * v_id / R);
+            const float u = __fdividef(1, detQ) * ((RM[8] - RM[5] * v_id / R) * (Ry / R * u_id - G.Dx) -
+                                                   (RM[2] - RM[5] * u_id / R) * (Ry / R * v_id - G.Dz));
+            const float v = __fdividef(1, detQ) * (-(RM[6] - RM[3] * v_id / R) * (Ry / R * u_id - G.Dx) +
+                                                   (RM[0] - RM[3] * u_id / R) * (Ry / R * v_id - G.Dz));
+            const float u_pix = u + (float)(G.Nu - 1) / 2.0f * G.du_mm * G.M;
+            const float v_pix = v + (float)(G.Nv - 1) / 2.0f * G.dv_mm * G.M;
+            const unsigned u_int = __float2uint_rd(u_pix);
+            const unsigned v_int = __float2uint_rd(v_pix);
+            const float u_weight = (u_pix - (float)u_int);
+            const float v_weight = (v_pix - (float)v_int);
+            if (u_pix >= 0.0 && u_pix <= (float)(G.Nu - 1) * G.du_mm * G.M && v_pix >= 0.0f &&
+                v_pix <= (float)(G.Nv - 1) * G.dv_mm * G.M) {
+                float t[4];
+                const size_t q00 = u_int + (size_t)v_int * G.Nu, q10 = u_int + 1 + (size_t)v_int * G.Nu;
+                const size_t q01 = u_int + (size_t)(v_int + 1) * G.Nu, q11 = u_int + 1 + (size_t)(v_int + 1) * G.Nu;
+                if (MODE == 1) {
+                    t[0] = q00 < npix ? 1.0f : 0.0f; t[1] = q10 < npix ? 1.0f : 0.0f;
+                    t[2] = q01 < npix ? 1.0f : 0.0f; t[3] = q11 < npix ? 1.0f : 0.0f;
+                } else {
+                    t[0] = q00 < npix ? __ldg(img + q00) : 0.0f; t[1] = q10 < npix ? __ldg(img + q10) : 0.0f;
+                    t[2] = q01 < npix ? __ldg(img + q01) : 0.0f; t[3] = q11 < npix ? __ldg(img + q11) : 0.0f;
+                }
+                acc = acc + __fdividef((t[0] * (1 - u_weight) + t[1] * u_weight) * (1 - v_weight) +
+                                           (t[2] * (1 - u_weight) + t[3] * u_weight) * v_weight,
+                                       (float)Nproj);
+            }
+        } else {
+            // geometric: Siddon angle sense, pixel units, taps inside the image
+            const float c = cospif(alpha / 180.0f), s = sinpif(alpha / 180.0f);
+            const float xa = xo * c - yo * s;
+            const float ya = xo * s + yo * c;
+            const float u_id = __fdividef(R * xa, ya + Rf);
+            const float v_id = __fdividef(R * zo, ya + Rf);
+            const float detQ = (RM[0] - RM[3] * u_id / R) * (RM[8] - RM[5] * v_id / R) -
+                               (RM[2] - RM[5] * u_id / R) * (RM[6] - RM[3] * v_id / R);
+            const float uu = __fdividef(1, detQ) * ((RM[8] - RM[5] * v_id / R) * (Ry / R * u_id - G.Dx) -
+                                                    (RM[2] - RM[5] * u_id / R) * (Ry / R * v_id - G.Dz));
+            const float vv = __fdividef(1, detQ) * (-(RM[6] - RM[3] * v_id / R) * (Ry / R * u_id - G.Dx) +
+                                                    (RM[0] - RM[3] * u_id / R) * (Ry / R * v_id - G.Dz));
+            const float u_pix = uu / (G.du_mm * G.M) + (float)(G.Nu - 1) * 0.5f;
+            const float v_pix = vv / (G.dv_mm * G.M) + (float)(G.Nv - 1) * 0.5f;
+            if (u_pix >= 0.0f && u_pix <= (float)(G.Nu - 1) && v_pix >= 0.0f && v_pix <= (float)(G.Nv - 1)) {
+                const int ui = min(max((int)floorf(u_pix), 0), G.Nu - 2);
+                const int vj = min(max((int)floorf(v_pix), 0), G.Nv - 2);
+                const float uw = u_pix - (float)ui, vw = v_pix - (float)vj;
+                float t00 = 1.0f, t10 = 1.0f, t01 = 1.0f, t11 = 1.0f;
+                if (MODE != 1) {
+                    t00 = tap<TEX>(img, tex, ui, vj, G.Nu);
+                    t10 = tap<TEX>(img, tex, ui + 1, vj, G.Nu);
+                    t01 = tap<TEX>(img, tex, ui, vj + 1, G.Nu);
+                    t11 = tap<TEX>(img, tex, ui + 1, vj + 1, G.Nu);
+                }
+                const float val = (t00 * (1.0f - uw) + t10 * uw) * (1.0f - vw) + (t01 * (1.0f - uw) + t11 * uw) * vw;
+                acc = acc + val / (float)Nproj;
+            }
+        }
+    }
+    if (MODE == 2) {
+        const float sv = sens[n];
+        const float f = vol[n];
+        vol[n] = (sv != 0.0f) ? __fdiv_rn(__fmul_rn(f, acc), sv) : 0.0f;
+    } else {
+        vol[n] = acc;
+    }
+}
+
+}  // namespace voxel
+
+// ---- host side ----------------------------------------------------------------------
+
+static voxel::VGeom vgeom(const Plan& P)
+{
+    voxel::VGeom G;
+    const recon_geometry_t& g = P.geom;
+    G.X = (int)g.vox.Xdim;
+    G.Y = (int)g.vox.Ydim;
+    G.Z = (int)g.vox.Zdim;
+    G.Nu = (int)g.det.NumAxPixels;
+    G.Nv = (int)g.det.NumTAxPixels;
+    G.vox[0] = g.vox.XVoxSize;
+    G.vox[1] = g.vox.YVoxSize;
+    G.vox[2] = g.vox.ZVoxSize;
+    G.R = g.cal.R;
+    G.Rf = g.cal.Rf;
+    G.Ry = g.cal.Ry;
+    G.Dx = g.cal.Dx;
+    G.Dz = g.cal.Dz;
+    G.M = g.cal.M;
+    G.du_mm = g.det.AxPixDimMm;
+    G.dv_mm = g.det.TAxPixDimMm;
+    for (int k = 0; k < 9; ++k) G.RM[k] = P.RM[k];
+    return G;
+}
+
+// Texture objects over the views of a device sinogram (pitched linear 2D
+// resources, point filtering, clamp addressing, unnormalised coordinates).
+// Returns false (no textures) when the base address or row pitch does not
+// meet the device's texture alignment; the caller then reads through the
+// read-only data path instead.
+static bool make_view_textures(const Plan& P, const float* sino, unsigned count, std::vector<cudaTextureObject_t>& out)
+{
+    int talign = 512, palign = 32;
+    cudaDeviceGetAttribute(&talign, cudaDevAttrTextureAlignment, P.device);
+    cudaDeviceGetAttribute(&palign, cudaDevAttrTexturePitchAlignment, P.device);
+    const size_t row = (size_t)P.geom.det.NumAxPixels * sizeof(float);
+    const size_t view_bytes = P.npix * sizeof(float);
+    if (row % (size_t)palign != 0) return false;
+    if (reinterpret_cast<uintptr_t>(sino) % (uintptr_t)talign != 0) return false;
+    if (count > 1 && view_bytes % (size_t)talign != 0) return false;
+    out.resize(count);
+    for (unsigned n = 0; n < count; ++n) {
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypePitch2D;
+        rd.res.pitch2D.devPtr = const_cast<float*>(sino) + (size_t)n * P.npix;
+        rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+        rd.res.pitch2D.width = P.geom.det.NumAxPixels;
+        rd.res.pitch2D.height = P.geom.det.NumTAxPixels;
+        rd.res.pitch2D.pitchInBytes = row;
+        cudaTextureDesc td{};
+        td.addressMode[0] = cudaAddressModeClamp;
+        td.addressMode[1] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModePoint;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        if (cudaCreateTextureObject(&out[n], &rd, &td, nullptr) != cudaSuccess) {
+            cudaGetLastError();
+            for (unsigned q = 0; q < n; ++q) cudaDestroyTextureObject(out[q]);
+            out.clear();
+            return false;
+        }
+    }
+    return true;
+}
+
+struct TexCache {
+    const float* base = nullptr;
+    unsigned count = 0;
+    cudaTextureObject_t* d_handles = nullptr;
+    std::vector<cudaTextureObject_t> handles;
+};
+static std::unordered_map<const Plan*, TexCache> g_tex_cache;
+
+static void release_textures(TexCache& c)
+{
+    for (auto h : c.handles) cudaDestroyTextureObject(h);
+    if (c.d_handles) cudaFree(c.d_handles);
+    c = TexCache{};
+}
+
+void release_plan_textures(const Plan* P)
+{
+    auto it = g_tex_cache.find(P);
+    if (it != g_tex_cache.end()) {
+        release_textures(it->second);
+        g_tex_cache.erase(it);
+    }
+}
+
+template <int VMODE, int MODE>
+static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angles, unsigned first, unsigned count,
+                                   unsigned Nproj, float* vol, const float* sens, bool cache_textures,
+                                   cudaStream_t s)
+{
+    voxel::VGeom G = vgeom(P);
+    dim3 blk(32, 4, 1), grid((G.X + 31) / 32, (G.Y + 3) / 4, G.Z);
+    bool tex = false;
+    cudaTextureObject_t* d_handles = nullptr;
+    std::vector<cudaTextureObject_t> local;
+    cudaTextureObject_t* d_local = nullptr;
+    if (VMODE == RECON_VOXEL_GEOMETRIC && MODE != 1 && sino) {
+        if (cache_textures) {
+            TexCache& c = g_tex_cache[&P];
+            if (c.base != sino || c.count != count) {
+                release_textures(c);
+                if (make_view_textures(P, sino, count, c.handles)) {
+                    RB_CUDA(cudaMalloc(&c.d_handles, count * sizeof(cudaTextureObject_t)));
+                    RB_CUDA(cudaMemcpy(c.d_handles, c.handles.data(), count * sizeof(cudaTextureObject_t),
+                                       cudaMemcpyHostToDevice));
+                    c.base = sino;
+                    c.count = count;
+                }
+            }
+            if (c.d_handles) {
+                tex = true;
+                d_handles = c.d_handles;
+            }
+        } else if (make_view_textures(P, sino, count, local)) {
+            RB_CUDA(cudaMalloc(&d_local, count * sizeof(cudaTextureObject_t)));
+            RB_CUDA(cudaMemcpyAsync(d_local, local.data(), count * sizeof(cudaTextureObject_t), cudaMemcpyHostToDevice,
+                                    s));
+            tex = true;
+            d_handles = d_local;
+        }
+    }
+    if (tex)
+        voxel::bp_kernel<VMODE, MODE, true><<<grid, blk, 0, s>>>(G, angles, first, count, Nproj, sino, d_handles, vol,
+                                                                  sens);
+    else
+        voxel::bp_kernel<VMODE, MODE, false><<<grid, blk, 0, s>>>(G, angles, first, count, Nproj, sino, nullptr, vol,
+                                                                   sens);
+    cudaError_t e = cudaGetLastError();
+    if (d_local) {
+        // the per-call textures must outlive the kernel
+        cudaStreamSynchronize(s);
+        for (auto h : local) cudaDestroyTextureObject(h);
+        cudaFree(d_local);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "voxel back projection launch");
+    return RECON_OK;
+}
+
+__global__ void voxel_set_angle_kernel(float* p, float v) { *p = v; }
+
+recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned count, bool scratch_slot,
+                        float angle_scratch, unsigned Nproj, int mode, bool ones, float* vol_accum,
+                        const float* sens, float* f_update, cudaStream_t s)
+{
+    if (scratch_slot) {
+        voxel_set_angle_kernel<<<1, 1, 0, s>>>(P.d_angles + P.nviews, angle_scratch);
+        first = P.nviews;
+        count = 1;
+    }
+    const bool ref = (mode == RECON_VOXEL_REFERENCE);
+    const bool cache = !scratch_slot;
+    if (ones) {
+        return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 1>(P, nullptr, P.d_angles, first, count, Nproj, vol_accum,
+                                                             nullptr, false, s)
+                   : launch_voxel<RECON_VOXEL_GEOMETRIC, 1>(P, nullptr, P.d_angles, first, count, Nproj, vol_accum,
+                                                             nullptr, false, s);
+    }
+    if (f_update) {
+        return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 2>(P, sino, P.d_angles, first, count, Nproj, f_update, sens,
+                                                             cache, s)
+                   : launch_voxel<RECON_VOXEL_GEOMETRIC, 2>(P, sino, P.d_angles, first, count, Nproj, f_update, sens,
+                                                             cache, s);
+    }
+    return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 0>(P, sino, P.d_angles, first, count, Nproj, vol_accum, nullptr,
+                                                         cache, s)
+               : launch_voxel<RECON_VOXEL_GEOMETRIC, 0>(P, sino, P.d_angles, first, count, Nproj, vol_accum, nullptr,
+                                                         cache, s);
+}
+
+}  // namespace rb

@@ -1,0 +1,182 @@
+"""COMPAT arithmetic on the GPU against the reference's own CUDA build and the oracle.
+
+The anchor is oracle/_ref/libref_gpu.so: the reference's sources
+(CT_Recon/siddon_kernelsMLEM.cuh, hf_siddon_class.hpp, hf_siddon_recon.hpp)
+compiled for sm_100a and driven through its own classes.  On the same GPU the
+per-ray set-up arrays, the per-step (voxel index, length) records and the
+forward projections must be bit-identical; back projections and MLEM differ
+only by the reference's float-atomic summation order (relative L2 <= 1e-5 per
+iteration, <= 1e-4 after the last).  Against the CPU oracle (IEEE division in
+place of __fdividef) the tolerance is relative L2 <= 1e-5.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2, small_cfg
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from oracle import oracle as O  # noqa: E402
+from recon_b200 import ARITH_COMPAT, Options, Plan  # noqa: E402
+from recon_b200.configs import CPU_SMALL, geom_dict  # noqa: E402
+
+REFG = O.ref_gpu()
+needs_ref = pytest.mark.skipif(REFG is None, reason="reference sm_100a build missing (oracle/_ref/libref_gpu.so)")
+
+GEOMS = {
+    "plain": small_cfg(),
+    "misaligned": small_cfg(Dx=0.7, Dz=-0.4, xangle=0.01, yangle=-0.02, zangle=0.015, Ry=803.0),
+    "z_parallel_row": small_cfg(Dz=0.75),
+    "cpu_small": dict(CPU_SMALL),
+}
+ANGLES = [0.0, 4.0, 37.0, 90.0, 133.0, 215.0, 359.0]
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def plan(cfg):
+    return Plan(cfg, Options(arith=ARITH_COMPAT))
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(GEOMS))
+def test_setup_bitexact_vs_reference_gpu(name):
+    cfg = GEOMS[name]
+    P = plan(cfg)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    for ang in ANGLES:
+        l1, a = P.compat_setup_view(ang)
+        l2, b = O.ref_gpu_setup_view(g, ang)
+        assert l1 == l2, (name, ang)
+        for k in a:
+            assert np.array_equal(bits(a[k]), bits(b[k])), (name, ang, k, int(np.sum(bits(a[k]) != bits(b[k]))))
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["plain", "misaligned", "cpu_small"])
+def test_trace_bitexact_vs_reference_gpu(name):
+    cfg = GEOMS[name]
+    P = plan(cfg)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    rng = np.random.default_rng(5)
+    for ang in (0.0, 37.0, 90.0, 215.0):
+        loopN = O.c_loopN(g, ang) + 8
+        rays = np.arange(g.npix, dtype=np.int32)
+        if len(rays) > 3000:
+            rays = np.sort(rng.choice(rays, 3000, replace=False)).astype(np.int32)
+        cap = loopN + 1
+        ridx = np.zeros(len(rays) * cap, np.int32)
+        rval = np.zeros(len(rays) * cap, np.float32)
+        lr = REFG.ref_gpu_trace(g, ang, len(rays), rays, cap, ridx, rval)
+        assert lr > 0
+        ln, idx, val = P.compat_trace(ang, rays, lr + 1)
+        assert ln == lr
+        ridx = ridx.reshape(len(rays), cap)[:, : lr + 1]
+        rval = rval.reshape(len(rays), cap)[:, : lr + 1]
+        assert np.array_equal(idx, ridx), (name, ang)
+        assert np.array_equal(bits(val), bits(rval)), (name, ang)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(GEOMS))
+def test_fp_bitexact_vs_reference_gpu(name):
+    cfg = GEOMS[name]
+    P = plan(cfg)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    vol = np.random.default_rng(6).random(g.nvox).astype(np.float32)
+    dvol = torch.from_numpy(vol).cuda().reshape(P.shape_vol)
+    for ang in ANGLES:
+        ref = np.zeros(g.npix, np.float32)
+        REFG.ref_gpu_fp_view(g, ang, vol, ref)
+        out = P.fp_view(dvol, ang).cpu().numpy().ravel()
+        assert np.array_equal(bits(out), bits(ref)), (name, ang, int(np.sum(bits(out) != bits(ref))))
+        assert rel_l2(out, O.c_fp_view(g, ang, vol)) < 1e-5
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(GEOMS))
+def test_bp_vs_reference_gpu(name):
+    cfg = GEOMS[name]
+    P = plan(cfg)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    img = np.random.default_rng(7).random(g.npix).astype(np.float32)
+    dimg = torch.from_numpy(img).cuda()
+    for ang in ANGLES[:4]:
+        ref = np.zeros(g.nvox, np.float32)
+        REFG.ref_gpu_bp_view(g, ang, img, ref)
+        out = P.bp_view(dimg, ang).cpu().numpy().ravel()
+        assert rel_l2(out, ref) < 1e-6, (name, ang)
+        assert rel_l2(out, O.c_bp_view(g, ang, img)) < 1e-5
+        again = P.bp_view(dimg, ang).cpu().numpy().ravel()
+        assert np.array_equal(bits(out), bits(again))  # deterministic
+
+
+def test_views_api_matches_single_view():
+    cfg = GEOMS["plain"]
+    P = plan(cfg)
+    vol = torch.rand(P.shape_vol, device="cuda")
+    sino = P.fp_views(vol)
+    for n in (0, 5, 11):
+        assert torch.equal(sino[n], P.fp_view(vol, P.angle(n)))
+    bp = P.bp_views(sino)
+    acc = torch.zeros_like(bp)
+    for n in range(P.nproj):
+        acc += P.bp_view(sino[n], P.angle(n))
+    assert rel_l2(bp.cpu().numpy(), acc.cpu().numpy()) < 1e-6
+
+
+def test_mlem_vs_oracle():
+    cfg = small_cfg(NumProj=12)
+    P = plan(cfg)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    rng = np.random.default_rng(8)
+    sino = (rng.random(12 * g.npix) * 3).astype(np.float32)
+    f_ref, s_ref, hist = O.c_mlem(g, 12, np.float32(cfg["DeltaAng"]), sino, 4, history=True)
+    dsino = torch.from_numpy(sino).cuda()
+    f = P.new_volume()
+    P.mlem_prepare()
+    torch.cuda.synchronize()
+    from recon_b200._lib import lib
+
+    f.fill_(1.0)
+    for it in range(4):
+        P.mlem_iteration(dsino, f)
+        err = rel_l2(f.cpu().numpy(), hist[it])
+        assert err < 1e-5 * (it + 1), (it, err)
+
+
+@needs_ref
+def test_mlem_from_cfg_vs_reference_driver(tmp_path):
+    """The reference's own a0_RECON_MLEM (file driven) against recon_mlem_from_cfg."""
+    from tests_helpers import write_case
+
+    cfg = small_cfg(NumProj=24, N_iteration=5)
+    folder = write_case(tmp_path, cfg, seed=9)
+    ref_dir = os.path.join(folder, "ref_out")
+    new_dir = os.path.join(folder, "new_out")
+    os.makedirs(ref_dir)
+    os.makedirs(new_dir)
+    from tests_helpers import write_cfg
+
+    write_cfg(os.path.join(folder, "ref.cfg"), cfg, folder, ref_dir + "/")
+    write_cfg(os.path.join(folder, "new.cfg"), cfg, folder, new_dir + "/")
+    ms = REFG.ref_gpu_mlem_cfg((folder + "/").encode(), b"ref.cfg")
+    assert ms > 0
+    from recon_b200 import mlem_from_cfg
+
+    mlem_from_cfg(folder, "new.cfg", Options(arith=ARITH_COMPAT))
+    n = cfg["Xdim"] * cfg["Ydim"] * cfg["Zdim"]
+    for it in range(5):
+        a = np.fromfile(os.path.join(new_dir, f"recon_{it}.bin"), np.float32)
+        b = np.fromfile(os.path.join(ref_dir, f"recon_{it}.bin"), np.float32)
+        assert a.size == n and b.size == n
+        assert rel_l2(a, b) < 1e-5 * (it + 1), (it, rel_l2(a, b))
+    assert os.path.exists(os.path.join(new_dir, "recon.info"))
