@@ -259,6 +259,11 @@ recon_status_t recon_compat_trace(recon_plan_t plan, float angle_deg, int nrays,
                                   int cap_steps, int* idx_out, float* len_out,
                                   unsigned int* loopN);
 
+/* loopN of a view: the largest per-ray step count delta_index of the
+ * reference's set-up (siddon_commons::a_calc_initial_limits,
+ * hf_siddon_class.hpp:93-106), for any plan.  Synchronous. */
+recon_status_t recon_view_step_count(recon_plan_t plan, float angle_deg, unsigned int* loopN);
+
 /* ---- file-driven drivers (the reference's siddon_recon entry points) ------ */
 
 /* siddon_recon::a0_RECON_MLEM(folder, cfg) (hf_siddon_recon.hpp:91-108):

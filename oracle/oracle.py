@@ -72,6 +72,7 @@ def lib():
             build_oracle()
         L = C.CDLL(path)
         L.orc_rotation_matrix.argtypes = [C.c_float, C.c_float, C.c_float, _f32p]
+        L.orc_c_set_device_model.argtypes = [C.c_int]
         L.orc_c_pixel_iterate2.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int]
         L.orc_c_pixel_iterate2.restype = C.c_float
         L.orc_c_setup_view.argtypes = [_GP, _f32p, C.c_float] + [_f32p] * 3 + [_u32p] + [_f32p] * 5 + [_u32p]
@@ -115,6 +116,7 @@ def ref_cpu():
         L.ref_cpu_trace.argtypes = [_GP, C.c_float, C.c_uint, C.c_int, _i32p, _i32p, _f32p]
         L.ref_cpu_mlem.argtypes = [_GP, C.c_uint, C.c_float, _u32p, _f32p, C.c_uint, _f32p, _f32p, C.c_void_p]
         L.ref_cpu_mlem_view.argtypes = [_GP, C.c_float, C.c_uint, _f32p, _f32p, _f32p]
+        L.ref_cpu_mlem_view_steps.argtypes = [_GP, C.c_float, C.c_uint, _f32p, _f32p, _f32p]
         _ref_cpu = L
     return _ref_cpu
 

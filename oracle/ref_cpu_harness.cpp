@@ -331,6 +331,23 @@ void ref_cpu_mlem(const orc_geom* g, unsigned NumProj, float DeltaAng, const uns
     if (sens_out) std::copy(sens.begin(), sens.end(), sens_out);
 }
 
+/* The first `steps` traversal steps of one view of one MLEM iteration (FP
+ * and BP each run `steps` of their loopN step launches, then their end
+ * segment), for timing: every step launches the same kernels over all rays
+ * and the full volume, so the time of a view scales as (loopN + 1) / (steps
+ * + 1) of this. */
+void ref_cpu_mlem_view_steps(const orc_geom* g, float angle, unsigned steps, const float* f_in,
+                             const float* gview, float* Ht_accum)
+{
+    RefState st(g);
+    st.limits(angle);
+    std::vector<float> img(st.Npix), gd(gview, gview + st.Npix), obj;
+    ref_cpu_fp_view(g, angle, steps, f_in, img.data());
+    launch(st.bimg, st.timg, [&] { divide1<float>(gd.data(), img.data()); });
+    bp_view(st, steps, gd.data(), obj);
+    launch(st.bobj, st.tobj, [&] { siddon_add_bp(Ht_accum, obj.data()); });
+}
+
 /* One view of one MLEM iteration (FP, ratio, BP, accumulate), the unit the
  * CPU baseline is timed on. */
 void ref_cpu_mlem_view(const orc_geom* g, float angle, unsigned loopN, const float* f_in,

@@ -108,6 +108,25 @@ static const union {
 } kNaN_bits = {0x7FFFFFFFu};
 #define kNaN (kNaN_bits.f)
 
+/* Two arithmetic models of the reference's FP32 kernels.
+ *   host (default): every operation rounded on its own and CUDART_NAN_F
+ *     stored into an unsigned mask as 0 -- what the reference's kernel
+ *     sources compute when compiled by a host compiler
+ *     (oracle/_ref/libref_cpu.so), against which this file is pinned bit for
+ *     bit;
+ *   device: what the reference's sm_100a build computes -- the
+ *     multiply-adds nvcc contracts are fused (fmaf) and the stores of
+ *     CUDART_NAN_F into unsigned masks are absent, so every mask stays 1.
+ *     Converting NaN to an integer is undefined behaviour in C++ and nvcc's
+ *     optimizer drops those stores (measured on oracle/_ref/libref_gpu.so:
+ *     mask = 1 for every ray of every geometry tested).  __fdividef remains
+ *     IEEE division here, so agreement with the device is close but not
+ *     bitwise. */
+static int g_device_model = 0;
+void orc_c_set_device_model(int on) { g_device_model = on ? 1 : 0; }
+#define MAD(a, b, c) (g_device_model ? fmaf((a), (b), (c)) : ((a) * (b) + (c)))
+#define MASK_CLEAR(m) do { if (!g_device_model) (m) = h_f2u(kNaN); } while (0)
+
 /* ------------------------------------------------------------------------- */
 /* Geometry shared by the FP32 restatement                                    */
 /* ------------------------------------------------------------------------- */
@@ -131,8 +150,8 @@ void orc_rotation_matrix(float tx, float ty, float tz, float RM[9])
  * to 1e-5 mm. */
 float orc_c_pixel_iterate2(float NumPixels, float PixelsDimMm, float Mag, int iterator)
 {
-    float result = h_fdividef(-(NumPixels - 1.0f), 2.0f) * PixelsDimMm * Mag +
-                   h_fdividef((float)iterator, NumPixels) * NumPixels * PixelsDimMm * Mag;
+    float result = MAD(h_fdividef(-(NumPixels - 1.0f), 2.0f) * PixelsDimMm, Mag,
+                       h_fdividef((float)iterator, NumPixels) * NumPixels * PixelsDimMm * Mag);
     return h_fdiv_rz(rintf(result * 100000.0f), 100000.0f);
 }
 
@@ -171,15 +190,15 @@ static void c_points12(const orc_geom* g, const float RM[9], const c_planes* P, 
     float dx = orc_c_pixel_iterate2((float)g->NumAxPixels, g->AxPixDimMm, g->M, u);
     float dy = g->R - g->Rf;
     float dz = orc_c_pixel_iterate2((float)g->NumTAxPixels, g->TAxPixDimMm, g->M, v);
-    dx = h_fdividef(g->R, (g->Ry + RM[3] * dx + RM[5] * dz)) * (RM[0] * dx + RM[2] * dz + g->Dx);
-    dz = h_fdividef(g->R, (g->Ry + RM[3] * dx + RM[5] * dz)) * (RM[6] * dx + RM[8] * dz + g->Dz);
+    dx = h_fdividef(g->R, MAD(RM[5], dz, MAD(RM[3], dx, g->Ry))) * (MAD(RM[0], dx, RM[2] * dz) + g->Dx);
+    dz = h_fdividef(g->R, MAD(RM[5], dz, MAD(RM[3], dx, g->Ry))) * (MAD(RM[6], dx, RM[8] * dz) + g->Dz);
     float c = h_cospif(h_fdividef(angle, 180.0f));
     float s = h_sinpif(h_fdividef(angle, 180.0f));
-    p1[0] = P->Xs[0] * c + P->Xs[1] * s;
-    p1[1] = -P->Xs[0] * s + P->Xs[1] * c;
+    p1[0] = MAD(P->Xs[0], c, P->Xs[1] * s);
+    p1[1] = MAD(-P->Xs[0], s, P->Xs[1] * c);
     p1[2] = P->Xs[2];
-    p2[0] = dx * c + dy * s;
-    p2[1] = -dx * s + dy * c;
+    p2[0] = MAD(dx, c, dy * s);
+    p2[1] = MAD(-dx, s, dy * c);
     p2[2] = dz;
 }
 
@@ -201,8 +220,8 @@ static float c_find_index(float index, float amin, float amax, float p1, float p
 {
     if (index > 0.0f) {
         float low = floorf(index), high = ceilf(index);
-        float plane_low = (plane1 + dplane * (low - 1.0f));
-        float plane_high = (plane1 + dplane * (high - 1.0f));
+        float plane_low = MAD(dplane, (low - 1.0f), plane1);
+        float plane_high = MAD(dplane, (high - 1.0f), plane1);
         float alow = h_fdividef(plane_low - p1, p2 - p1);
         float ahigh = h_fdividef(plane_high - p1, p2 - p1);
         if (alow >= amin && alow <= amax) return low;
@@ -218,7 +237,7 @@ static void c_bound_index(float* imin, float* imax, uint32_t* mask)
     if ((*imax - *imin) < 0 && *imin <= 1 && *imax <= 1) {
         *imin = 0;
         *imax = 0;
-        *mask = h_f2u(kNaN);
+        MASK_CLEAR(*mask);
     }
 }
 
@@ -229,10 +248,10 @@ static float c_alpha_float(uint32_t mn, uint32_t mx, float p1, float p2, float p
 {
     float plane;
     if ((p2 - p1) > 0 && (mx - mn) > 0) {
-        plane = plane1 + dplane * ((float)mn - 1.0f);
+        plane = MAD(dplane, ((float)mn - 1.0f), plane1);
         return h_fdividef(plane - p1, p2 - p1);
     } else if ((p2 - p1) < 0 && (mx - mn) > 0) {
-        plane = plane1 + dplane * ((float)mx - 1.0f);
+        plane = MAD(dplane, ((float)mx - 1.0f), plane1);
         return h_fdividef(plane - p1, p2 - p1);
     }
     return kNaN;
@@ -245,15 +264,15 @@ static uint32_t c_calc_indices(float* ai, float* af, uint32_t* mask, float p1, f
 {
     float ix, iy;
     if ((p2 - p1) > 0) {
-        ix = Nplanes - h_fdividef((plane2 - amin * (p2 - p1) - p1), dplane);
-        iy = 1.0f + h_fdividef((p1 + amax * (p2 - p1) - plane1), dplane);
+        ix = Nplanes - h_fdividef((MAD(-amin, (p2 - p1), plane2) - p1), dplane);
+        iy = 1.0f + h_fdividef((MAD(amax, (p2 - p1), p1) - plane1), dplane);
     } else if ((p2 - p1) < 0) {
-        ix = Nplanes - h_fdividef((plane2 - amax * (p2 - p1) - p1), dplane);
-        iy = 1.0f + h_fdividef((p1 + amin * (p2 - p1) - plane1), dplane);
+        ix = Nplanes - h_fdividef((MAD(-amax, (p2 - p1), plane2) - p1), dplane);
+        iy = 1.0f + h_fdividef((MAD(amin, (p2 - p1), p1) - plane1), dplane);
     } else {
         ix = 0;
         iy = 0;
-        *mask = h_f2u(kNaN);
+        MASK_CLEAR(*mask);
     }
     ix = (float)*mask * c_find_index(ix, amin, amax, p1, p2, plane1, dplane);
     iy = (float)*mask * c_find_index(iy, amin, amax, p1, p2, plane1, dplane);
@@ -270,15 +289,15 @@ static void c_ray_setup(const orc_geom* g, const float RM[9], const c_planes* P,
     float* p1 = r->p1;
     float* p2 = r->p2;
     c_points12(g, RM, P, u, v, angle, p1, p2);
-    r->d12 = sqrtf((p2[0] - p1[0]) * (p2[0] - p1[0]) + (p2[1] - p1[1]) * (p2[1] - p1[1]) +
-                   (p2[2] - p1[2]) * (p2[2] - p1[2]));
+    r->d12 = sqrtf(MAD((p2[2] - p1[2]), (p2[2] - p1[2]),
+                       MAD((p2[0] - p1[0]), (p2[0] - p1[0]), (p2[1] - p1[1]) * (p2[1] - p1[1]))));
     float ax[2], ay[2], az[2];
     c_alpha_1N(p1[0], p2[0], P->Pi[0], P->Pf[0], ax);
     c_alpha_1N(p1[1], p2[1], P->Pi[1], P->Pf[1], ay);
     c_alpha_1N(p1[2], p2[2], P->Pi[2], P->Pf[2], az);
     float amin = fmaxf(fmaxf(fmaxf(0, fminf(ax[0], ax[1])), fminf(ay[0], ay[1])), fminf(az[0], az[1]));
     float amax = fminf(fminf(fminf(1, fmaxf(ax[0], ax[1])), fmaxf(ay[0], ay[1])), fmaxf(az[0], az[1]));
-    uint32_t mask = (amax <= amin) ? h_f2u(kNaN) : 1u; /* calc_mask :88-98 */
+    uint32_t mask = (amax <= amin && !g_device_model) ? h_f2u(kNaN) : 1u; /* calc_mask :88-98 */
     amin = (float)mask * amin;
     amax = (float)mask * amax;
     uint32_t idx[3];
@@ -409,9 +428,9 @@ static int32_t c_segment(const orc_geom* g, const c_planes* P, const orc_c_ray* 
     if (a_hi > a_lo) {
         float mid = h_fdividef((a_hi + a_lo), 2.0f);
         rl = r->d12 * (a_hi - a_lo);
-        ix = h_f2i_rz((h_fdividef((r->p1[0] + mid * (r->p2[0] - r->p1[0]) - P->Pi[0]), P->Pd[0])));
-        iy = h_f2i_rz((h_fdividef((r->p1[1] + mid * (r->p2[1] - r->p1[1]) - P->Pi[1]), P->Pd[1])));
-        iz = h_f2i_rz((h_fdividef((r->p1[2] + mid * (r->p2[2] - r->p1[2]) - P->Pi[2]), P->Pd[2])));
+        ix = h_f2i_rz((h_fdividef((MAD(mid, (r->p2[0] - r->p1[0]), r->p1[0]) - P->Pi[0]), P->Pd[0])));
+        iy = h_f2i_rz((h_fdividef((MAD(mid, (r->p2[1] - r->p1[1]), r->p1[1]) - P->Pi[1]), P->Pd[1])));
+        iz = h_f2i_rz((h_fdividef((MAD(mid, (r->p2[2] - r->p1[2]), r->p1[2]) - P->Pi[2]), P->Pd[2])));
     }
     *len = rl;
     if (ix >= 0 && ix < (int32_t)g->Xdim && iy >= 0 && iy < (int32_t)g->Ydim && iz >= 0 &&

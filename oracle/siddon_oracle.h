@@ -61,6 +61,8 @@ typedef struct {
 
 /* ---- FP32 compat restatement ---- */
 void orc_rotation_matrix(float xangle, float yangle, float zangle, float RM[9]);
+/* 0: host model (default), 1: device model -- see siddon_oracle.c */
+void orc_c_set_device_model(int on);
 float orc_c_pixel_iterate2(float NumPixels, float PixelsDimMm, float Mag, int iterator);
 void orc_c_ray_setup(const orc_geom* g, const float RM[9], float angle_deg, int u, int v,
                      orc_c_ray* out);

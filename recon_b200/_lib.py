@@ -107,6 +107,7 @@ def lib() -> C.CDLL:
         "recon_mlem_update": (st, [P, P, P, P]),
         "recon_mlem_backward_update": (st, [P, P, P]),
         "recon_count_intersections": (st, [P, C.POINTER(C.c_ulonglong)]),
+        "recon_view_step_count": (st, [P, f, up]),
         "recon_set_ones": (st, [P, C.c_size_t, P]),
         "recon_divide1": (st, [P, P, C.c_size_t, P]),
         "recon_multiply1": (st, [P, P, C.c_size_t, P]),
@@ -135,7 +136,7 @@ def exported_symbols() -> list[str]:
         "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_set_ones", "recon_divide1", "recon_multiply1",
-        "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_mlem_from_cfg",
+        "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_view_step_count", "recon_mlem_from_cfg",
         "recon_forward_projection_from_cfg", "recon_backward_projection_from_cfg",
     ]
 

@@ -258,6 +258,7 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
         RB_CHECK(P->alloc(&P->d_angles, nv1, "angles"));
         RB_CUDA(cudaMemcpy(P->d_angles, P->view_angles.data(), nv1 * sizeof(float), cudaMemcpyHostToDevice));
         RB_CHECK(P->alloc(&P->d_view_img, P->npix, "view image"));
+        RB_CHECK(P->alloc(&P->d_loopN, nv1, "loopN"));
         if (opt.arith == RECON_ARITH_EXACT) {
             RB_CHECK(P->alloc(&P->d_txy, nv1 * geom->det.NumAxPixels, "ray table xy"));
             RB_CHECK(P->alloc(&P->d_kxy, nv1 * geom->det.NumAxPixels, "ray table kc"));
@@ -266,7 +267,6 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_w, P->npix, "ray weights"));
             RB_CHECK(build_exact_tables(*P, 0));
         } else {
-            RB_CHECK(P->alloc(&P->d_loopN, nv1, "loopN"));
             RB_CHECK(P->alloc(&P->d_maxabs, nv1, "maxabs"));
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));
             RB_CHECK(P->alloc(&P->d_ht, P->nvox, "Ht"));
@@ -442,6 +442,15 @@ recon_status_t recon_mlem_backward_update(recon_plan_t P, float* d_f, void* stre
     RB_CHECK(use_device(*P));
     return exact_bp(*P, P->d_ratio, true, P->opt.sino == RECON_SINO_BF16, 0, P->nviews, false, false, nullptr,
                     P->d_sens, d_f, as_stream(stream));
+}
+
+recon_status_t recon_view_step_count(recon_plan_t P, float angle, unsigned* loopN)
+{
+    if (!P || !loopN) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    RB_CHECK(use_device(*P));
+    RB_CHECK(compat_view_loopN(*P, angle, P->nviews, 0));
+    RB_CUDA(cudaMemcpy(loopN, P->d_loopN + P->nviews, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return RECON_OK;
 }
 
 recon_status_t recon_count_intersections(recon_plan_t P, unsigned long long* count)

@@ -12,10 +12,16 @@
 // reference's own: every expression below keeps the operand order of the
 // reference line it restates, so that the compiler forms the same FMAs and
 // the intrinsics (__fdividef, __fdiv_rz, cospif, sinpif, __float2int_rz) see
-// the same operands.  Float-to-unsigned conversions the reference makes
-// implicitly (CUDART_NAN_F stored to an unsigned, float indices passed as
-// unsigned) are made explicit with the saturating device conversion, which
-// is what the hardware does for them (NaN -> 0).
+// the same operands.  Float-to-unsigned conversions of run-time values
+// (float plane indices passed as unsigned) are made explicit with the
+// saturating device conversion (NaN -> 0), which is what the hardware does.
+// The reference also stores the constant CUDART_NAN_F into its unsigned
+// ray mask (calc_mask, the parallel-axis branch of siddon_calc_indices,
+// bound_index).  Converting NaN to an integer is undefined behaviour in C++,
+// and nvcc's optimizer drops those stores: the reference's sm_100a build
+// keeps mask = 1 for every ray (measured on all test geometries, misses and
+// axis-parallel rays included).  COMPAT reproduces the GPU build, so the mask
+// is never cleared here either.
 //
 // Back projection keeps the reference's ray-driven scatter, but accumulates
 // each view's contributions len*img in 64-bit fixed point (integer atomics,
@@ -93,15 +99,13 @@ __device__ __forceinline__ unsigned axis_indices(float& ai, float& af, unsigned&
         iy = 1.0f + __fdividef((p1 + amin * (p2 - p1) - plane1), dplane);
     } else {
         ix = 0;
-        iy = 0;
-        mask = 0u;  // CUDART_NAN_F stored to unsigned
+        iy = 0;  // (the reference's mask store here is dropped by nvcc)
     }
     ix = (float)mask * plane_index(ix, amin, amax, p1, p2, plane1, dplane);
     iy = (float)mask * plane_index(iy, amin, amax, p1, p2, plane1, dplane);
     if ((iy - ix) < 0 && ix <= 1 && iy <= 1) {
         ix = 0;
-        iy = 0;
-        mask = 0u;
+        iy = 0;  // bound_index; its mask store is dropped likewise
     }
     ai = (float)mask * plane_alpha(__float2uint_rz(ix), __float2uint_rz(iy), p1, p2, plane1, dplane);
     af = (float)mask * plane_alpha(__float2uint_rz(iy), __float2uint_rz(ix), p1, p2, plane1, dplane);
@@ -139,7 +143,7 @@ __device__ __forceinline__ void setup(const CompatGeom& G, float angle, int u, i
     }
     float amin = fmaxf(fmaxf(fmaxf(0, fminf(a1[0], aN[0])), fminf(a1[1], aN[1])), fminf(a1[2], aN[2]));
     float amax = fminf(fminf(fminf(1, fmaxf(a1[0], aN[0])), fmaxf(a1[1], aN[1])), fmaxf(a1[2], aN[2]));
-    unsigned mask = (amax <= amin) ? 0u : 1u;  // calc_mask (:88-98)
+    unsigned mask = 1u;  // calc_mask (:88-98) as the GPU build evaluates it
     amin = (float)mask * amin;
     amax = (float)mask * amax;
     unsigned idx[3];

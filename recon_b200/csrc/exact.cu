@@ -212,19 +212,18 @@ __global__ void __launch_bounds__(128) fp_kernel(ExactGeom G, const float4* __re
                 acc = fmaf(L, fv, acc);
             }
             cur = m;
-            if (tx == m) {
-                kx += fdx;
-                tx = fmaf(kx, T.x, T.y);
-                idx += sx;
-            } else if (ty == m) {
-                ky += fdy;
-                ty = fmaf(ky, T.z, T.w);
-                idx += sy;
-            } else {
-                kz += fdz;
-                tz = fmaf(kz, Z.S, Z.O);
-                idx += sz;
-            }
+            // advance the axis whose plane was crossed (x before y before z
+            // on ties), without divergent branches
+            const bool bx = (tx == m);
+            const bool by = !bx && (ty == m);
+            const bool bz = !bx && !by;
+            kx = bx ? kx + fdx : kx;
+            ky = by ? ky + fdy : ky;
+            kz = bz ? kz + fdz : kz;
+            tx = bx ? fmaf(kx, T.x, T.y) : tx;
+            ty = by ? fmaf(ky, T.z, T.w) : ty;
+            tz = bz ? fmaf(kz, Z.S, Z.O) : tz;
+            idx += bx ? sx : (by ? sy : sz);
         }
     }
     const float hf = w * acc;
@@ -252,10 +251,14 @@ __global__ void __launch_bounds__(128) bp_kernel(ExactGeom G, const float4* __re
                                                   float* __restrict__ vol, const float* __restrict__ sens)
 {
     extern __shared__ float smem[];
-    float* acc = smem;                                       // [ZC][128]
-    ZParam* szp = reinterpret_cast<ZParam*>(smem + ZC * 128);  // [Nv]
+    float* acc = smem;                                         // [ZC][128]
+    float4* szb = reinterpret_cast<float4*>(smem + ZC * 128);  // [Nv] mirrored z planes
     const int tid = threadIdx.x + threadIdx.y * 32;
-    for (int q = tid; q < G.Nv; q += 128) szp[q] = zp[q];
+    for (int q = tid; q < G.Nv; q += 128) {
+        const ZParam z = zp[q];
+        const bool pos = z.S > 0.0f;
+        szb[q] = make_float4(fabsf(z.S), pos ? z.O : -z.O, (float)z.kc, pos ? 1.0f : -1.0f);
+    }
 #pragma unroll
     for (int q = 0; q < ZC; ++q) acc[q * 128 + tid] = 0.0f;
     __syncthreads();
@@ -280,7 +283,7 @@ __global__ void __launch_bounds__(128) bp_kernel(ExactGeom G, const float4* __re
             for (int c4 = 0; c4 < 4; ++c4) {
                 const float X = (c4 & 1) ? Xb : Xa, Y = (c4 & 2) ? Yb : Ya;
                 const float xv = X * CS.x - Y * CS.y, yv = X * CS.y + Y * CS.x;
-                const float ud = G.R * xv / (yv + G.Rf) * RyR - G.Dx;
+                const float ud = __fdividef(G.R * xv, yv + G.Rf) * RyR - G.Dx;  // candidates only
                 const float uf = (ud - G.ud0) * inv_du;
                 umin = fminf(umin, uf);
                 umax = fmaxf(umax, uf);
@@ -295,9 +298,9 @@ __global__ void __launch_bounds__(128) bp_kernel(ExactGeom G, const float4* __re
                 const float A = fmaxf(fminf(xa, xb), fminf(ya, yb));
                 const float B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
                 if (!(A < B)) continue;
-                // rows v whose ray can cross the z-chunk inside [A, B]:
-                // z = vd * (t + Rf) / R  =>  vd = z * R / (t + Rf)
-                const float ra = G.R / (A + G.Rf), rb = G.R / (B + G.Rf);
+                // rows v whose ray can cross the z-chunk inside [A, B]
+                // (candidates only, with a margin): z = vd * (t + Rf) / R
+                const float ra = __fdividef(G.R, A + G.Rf), rb = __fdividef(G.R, B + G.Rf);
                 const float c1 = Za * ra, c2 = Za * rb, c3 = Zb * ra, c4 = Zb * rb;
                 const float vdmin = fminf(fminf(c1, c2), fminf(c3, c4));
                 const float vdmax = fmaxf(fmaxf(c1, c2), fmaxf(c3, c4));
@@ -306,37 +309,40 @@ __global__ void __launch_bounds__(128) bp_kernel(ExactGeom G, const float4* __re
                 const int v_lo = max(0, (int)ceilf(fminf(vfa, vfb) - 2e-3f));
                 const int v_hi = min(G.Nv - 1, (int)floorf(fmaxf(vfa, vfb) + 2e-3f));
                 const ST* srow = sino + ((size_t)vi * G.Nv) * G.Nu + u;
+                // Sweep the needles (the rays' pieces inside this column) in
+                // increasing z together with the chunk's voxels.  The lowest
+                // voxel a needle touches never decreases from one needle to
+                // the next, so k carries over.  Each ray's z planes are
+                // mirrored (t -> -t for rays going down, exact in IEEE) so
+                // that T(k) increases with k for every ray:
+                //   L(v, k) = min(B', T(k+1)) - max(A', T(k)).
+                int k = k0;
                 for (int v = v_lo; v <= v_hi; ++v) {
-                    const ZParam Z = szp[v];
-                    // z voxel containing t = A, then walk toward larger t
-                    const int up = Z.S > 0.0f ? 1 : -1;
-                    int k = (int)floorf(fmaf(A - Z.O, Z.inv_S, (float)Z.kc));
-#pragma unroll 1
-                    for (int it = 0; it < 4; ++it) {
-                        float t0 = plane_t(k, Z.S, Z.O, Z.kc), t1 = plane_t(k + 1, Z.S, Z.O, Z.kc);
-                        if (A < fminf(t0, t1)) k -= up;
-                        else if (A >= fmaxf(t0, t1)) k += up;
-                        else break;
-                    }
-                    // first voxel of the chunk along the walk
-                    if (up > 0) k = max(k, k0);
-                    else k = min(k, k1 - 1);
+                    const float4 Z = szb[v];  // {|S|, sign(S)*O, kc, sign(S)}
                     float val;
                     if (MODE == 1) val = __ldg(wtab + (size_t)v * G.Nu + u);
                     else val = load_val<ST>(srow + (size_t)v * G.Nu);
                     if (WEIGHTED && MODE != 1) val *= __ldg(wtab + (size_t)v * G.Nu + u);
+                    const float Ap = Z.w > 0.0f ? A : -B;
+                    const float Bp = Z.w > 0.0f ? B : -A;
+                    float kf = (float)k;
+                    float T1 = fmaf(kf + 1.0f - Z.z, Z.x, Z.y);
+                    while (T1 <= Ap && k < k1) {  // voxel k lies wholly before the needle
+                        ++k;
+                        kf += 1.0f;
+                        T1 = fmaf(kf + 1.0f - Z.z, Z.x, Z.y);
+                    }
+                    if (k >= k1) break;  // this and every later needle lie above the chunk
+                    float T0 = fmaf(kf - Z.z, Z.x, Z.y);
+                    float* a = acc + (k - k0) * 128 + tid;
 #pragma unroll 1
-                    while (k >= k0 && k < k1) {
-                        const float t0 = plane_t(k, Z.S, Z.O, Z.kc), t1 = plane_t(k + 1, Z.S, Z.O, Z.kc);
-                        const float lo = fminf(t0, t1), hi = fmaxf(t0, t1);
-                        if (lo >= B) break;
-                        const float L = fminf(B, hi) - fmaxf(A, lo);
-                        if (L > 0.0f) {
-                            float* a = acc + (k - k0) * 128 + tid;
-                            *a = fmaf(L, val, *a);
-                        }
-                        if (hi >= B) break;
-                        k += up;
+                    for (int kk = k;;) {
+                        const float L = fminf(Bp, T1) - fmaxf(Ap, T0);
+                        if (L > 0.0f) *a = fmaf(L, val, *a);
+                        if (T1 >= Bp || ++kk >= k1) break;
+                        a += 128;
+                        T0 = T1;
+                        T1 = fmaf((float)kk + 1.0f - Z.z, Z.x, Z.y);
                     }
                 }
             }

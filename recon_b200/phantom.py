@@ -77,9 +77,17 @@ def phantom(cfg: dict, seed: int | None = None, n_ellipsoids: int | None = None,
     return vol
 
 
-def noisy(p, I0: float, seed: int):
+def noisy(p, I0: float, seed: int, clip: bool = True):
     """g = ln(I0 / max(Poisson(I0 * exp(-p)), 1)) for line integrals p
-    (numpy array, or torch tensor -- then sampled on its device)."""
+    (numpy array, or torch tensor -- then sampled on its device).
+
+    With ``clip`` (the default) negative values -- rays through air whose
+    photon count exceeds I0 -- are set to 0.  Line integrals are non-negative,
+    and MLEM's multiplicative update keeps the image non-negative only for
+    non-negative data: with the raw values MLEM goes negative at air voxels
+    and becomes chaotic (in FP64, a 1e-7 relative data perturbation grows to
+    a 0.26 relative image difference by iteration 10 on a 48x48x40, 45-view
+    case), so no FP32 result can track an FP64 one there."""
     try:
         import torch
 
@@ -88,10 +96,16 @@ def noisy(p, I0: float, seed: int):
             gen.manual_seed(int(seed))
             lam = float(I0) * torch.exp(-p.double())
             counts = torch.poisson(lam, generator=gen).clamp_min(1.0)
-            return torch.log(float(I0) / counts).to(torch.float32)
+            g = torch.log(float(I0) / counts)
+            if clip:
+                g = g.clamp_min(0.0)
+            return g.to(torch.float32)
     except ImportError:
         pass
     rng = np.random.default_rng(seed)
     lam = float(I0) * np.exp(-np.asarray(p, np.float64))
     counts = np.maximum(rng.poisson(lam), 1).astype(np.float64)
-    return np.log(float(I0) / counts).astype(np.float32)
+    g = np.log(float(I0) / counts)
+    if clip:
+        g = np.maximum(g, 0.0)
+    return g.astype(np.float32)
