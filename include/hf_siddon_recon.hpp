@@ -24,10 +24,12 @@
 
 class siddon_recon : public forward, public backward {
 public:
-    void a0_RECON_MLEM(std::string configurationfilename, std::string outputparameterfilename)
+    // Declared (configurationfilename, outputparameterfilename) in the
+    // reference but defined and used as (folder, file name)
+    // (hf_siddon_recon.hpp:91-108, mlem.cu:32); the definition is what runs.
+    void a0_RECON_MLEM(std::string configurationfilefolder, std::string configurationfilename)
     {
-        (void)outputparameterfilename;
-        run_mlem("", configurationfilename);
+        run_mlem(configurationfilefolder, configurationfilename);
     }
     void a0_RECON_MLEM(std::string configurationfilename) { run_mlem("", configurationfilename); }
     void a0_RECON_MLEM(std::string configurationfilefolder, std::string configurationfilename,

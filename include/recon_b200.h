@@ -222,6 +222,26 @@ recon_status_t recon_mlem_update(recon_plan_t plan, float* d_f, const float* d_h
  * recon_mlem_forward(all views) followed by this is one recon_mlem_iteration. */
 recon_status_t recon_mlem_backward_update(recon_plan_t plan, float* d_f, void* stream);
 
+/* ---- batches of independent reconstructions ------------------------------ */
+
+/* Many MLEM problems (each its own geometry) run together: every iteration of
+ * every problem is two persistent kernels pulling tiles of all problems from
+ * one work queue, replayed as a CUDA graph.  The reference has no batch entry
+ * point; it is the loop a user writes around siddon_recon::a0_RECON_MLEM
+ * (hf_siddon_recon.hpp:91-108) over many scans.  Each problem's result is
+ * bit-identical to recon_mlem on a plan of the same geometry and options.
+ * EXACT arithmetic, Siddon back projector, FP32 sinograms only. */
+typedef struct recon_batch* recon_batch_t;
+recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const recon_options_t* opt,
+                                  recon_batch_t* batch);
+void recon_batch_destroy(recon_batch_t batch);
+/* d_g[p] / d_f[p]: problem p's sinogram [NumProj][Nv][Nu] and image
+ * [Z][Y][X] on the batch's device.  The first call times a few candidate
+ * launch shapes on the caller's data (the images are restored) and
+ * synchronises; later calls are asynchronous on `stream`. */
+recon_status_t recon_batch_mlem(recon_batch_t batch, const float* const* d_g, float* const* d_f,
+                                unsigned int iters, int init_ones, void* stream);
+
 /* Number of (ray, voxel) pairs with positive intersection length over all
  * NumProj views (EXACT arithmetic): the I of the throughput figure
  * "ray-voxel intersections per second".  Synchronous. */

@@ -117,6 +117,9 @@ def lib() -> C.CDLL:
         "recon_mlem_from_cfg": (st, [C.c_char_p, C.c_char_p, C.POINTER(Options)]),
         "recon_forward_projection_from_cfg": (st, [C.c_char_p, C.c_char_p, C.POINTER(Options)]),
         "recon_backward_projection_from_cfg": (st, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(Options)]),
+        "recon_batch_create": (st, [C.POINTER(Geometry), C.c_int, C.POINTER(Options), C.POINTER(P)]),
+        "recon_batch_destroy": (None, [P]),
+        "recon_batch_mlem": (st, [P, C.POINTER(P), C.POINTER(P), u, C.c_int, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name, None)
@@ -137,7 +140,8 @@ def exported_symbols() -> list[str]:
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_set_ones", "recon_divide1", "recon_multiply1",
         "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_view_step_count", "recon_mlem_from_cfg",
-        "recon_forward_projection_from_cfg", "recon_backward_projection_from_cfg",
+        "recon_forward_projection_from_cfg", "recon_backward_projection_from_cfg", "recon_batch_create",
+        "recon_batch_destroy", "recon_batch_mlem",
     ]
 
 

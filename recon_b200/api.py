@@ -230,6 +230,60 @@ class Plan:
         return int(loopN.value), idx.reshape(len(rays), cap_steps), ln.reshape(len(rays), cap_steps)
 
 
+class Batch:
+    """Many independent MLEM reconstructions run together (recon_batch_*).
+
+    Each problem has its own geometry; every iteration of every problem is two
+    persistent kernels over one work queue.  The reference has no batch call:
+    this replaces a loop of siddon_recon::a0_RECON_MLEM over many scans.
+    """
+
+    def __init__(self, cfgs: list[dict], options: Options | None = None):
+        self.cfgs = [dict(c) for c in cfgs]
+        self.options = options or Options()
+        geoms = (L.Geometry * len(cfgs))(*[geometry(c) for c in cfgs])
+        h = C.c_void_p()
+        check(lib().recon_batch_create(geoms, len(cfgs), C.byref(self.options.c()), C.byref(h)))
+        self._h = h
+        self.shapes_vol = [(int(c["Zdim"]), int(c["Ydim"]), int(c["Xdim"])) for c in cfgs]
+        self.shapes_sino = [(int(c["NumProj"]), int(c["TAxPixels"]), int(c["AxPixels"])) for c in cfgs]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().recon_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return len(self.cfgs)
+
+    def new_volumes(self, fill: float = 0.0):
+        import torch
+
+        dev = torch.device("cuda", self.options.device)
+        return [torch.full(s, fill, dtype=torch.float32, device=dev) for s in self.shapes_vol]
+
+    def mlem(self, gs, iters: int, fs=None, init_ones: bool = True):
+        """Run `iters` iterations of every problem; gs[p] is problem p's sinogram."""
+        if len(gs) != len(self.cfgs):
+            raise ValueError(f"expected {len(self.cfgs)} sinograms, got {len(gs)}")
+        fs = self.new_volumes() if fs is None else fs
+        for p, (g, f) in enumerate(zip(gs, fs)):
+            if tuple(g.shape) != self.shapes_sino[p] or tuple(f.shape) != self.shapes_vol[p]:
+                raise ValueError(f"problem {p}: sinogram {tuple(g.shape)} / image {tuple(f.shape)} do not match "
+                                 f"{self.shapes_sino[p]} / {self.shapes_vol[p]}")
+        n = len(self.cfgs)
+        gp = (C.c_void_p * n)(*[_ptr(g) for g in gs])
+        fp = (C.c_void_p * n)(*[_ptr(f) for f in fs])
+        check(lib().recon_batch_mlem(self._h, gp, fp, int(iters), 1 if init_ones else 0, _stream()))
+        return fs
+
+
 def mlem_from_cfg(folder: str, cfg: str, options: Options | None = None) -> None:
     """siddon_recon::a0_RECON_MLEM(folder, cfg) (hf_siddon_recon.hpp:91-108)."""
     o = (options or Options()).c()
