@@ -70,7 +70,10 @@ def batched_problems(n: int = 48, seed: int = 4, iters: int = 20) -> list[dict]:
     1e4..1e6 (log-uniform).  Every dimension is a multiple of 4 (the reference
     launches 4-wide blocks with no bounds checks).  Rf = 500 mm.  Voxel size:
     the largest volume axis spans 0.8 of the field of view at isocentre,
-    ``vox = 0.8 * (Nu * pitch * Rf / SDD) / max(X, Y, Z)``, with a 1 mm pitch.
+    ``vox = 0.8 * (Nu * pitch * Rf / SDD) / max(X, Y, Z)``, with a 1 mm pitch,
+    reduced where needed so that the volume's bounding sphere stays within
+    0.9 of the isocentre-to-detector distance (SDD - Rf): the detector must
+    not cut through the object.
     """
     import numpy as np
 
@@ -84,6 +87,8 @@ def batched_problems(n: int = 48, seed: int = 4, iters: int = 20) -> list[dict]:
         I0 = float(10.0 ** rng.uniform(4.0, 6.0))
         pitch = 1.0
         vox = 0.8 * (Nu * pitch * 500.0 / sdd) / max(X, Y, Z)
+        half_diag = 0.5 * float(np.sqrt(X * X + Y * Y + Z * Z))
+        vox = min(vox, 0.9 * min(500.0, sdd - 500.0) / half_diag)
         vox = float(np.float32(round(vox, 4)))
         c = _cfg((X, Y, Z), vox, (Nu, Nu), pitch, nproj, iters, n_ellipsoids=10, I0=I0, seed=1000 + i)
         c["R"] = c["Ry"] = float(np.float32(round(sdd, 2)))

@@ -92,8 +92,9 @@ def test_batch_of_generated_problems():
 def test_batch_rejects_unsupported_and_mismatched():
     with pytest.raises(ReconError):
         Batch(MIXED[:1], Options(arith=ARITH_COMPAT))
-    B = Batch(MIXED[:2])
-    gs = _sinos(MIXED[:2], 9)
+    pair = [MIXED[0], MIXED[2]]  # different volume and detector shapes
+    B = Batch(pair)
+    gs = _sinos(pair, 9)
     with pytest.raises(ValueError):
         B.mlem(gs[:1], 1)
     with pytest.raises(ValueError):
