@@ -284,6 +284,24 @@ recon_status_t recon_compat_trace(recon_plan_t plan, float angle_deg, int nrays,
  * hf_siddon_class.hpp:93-106), for any plan.  Synchronous. */
 recon_status_t recon_view_step_count(recon_plan_t plan, float angle_deg, unsigned int* loopN);
 
+/* ---- allocation-free back projection ------------------------------------ */
+
+/* COMPAT back projection of one view without any device allocation, for
+ * callers that may not allocate device memory (no plan is needed): d_vol =
+ * BP(d_img) at angle_deg, bit-identical to recon_bp_view on a COMPAT plan of
+ * the same geometry.  No reference counterpart: the reference's backward
+ * class allocates its buffers in a1_Binitiate (hf_siddon_class.hpp).
+ * Device state lives in one static scratch array per device (about 16 MiB):
+ *  - volumes above RECON_NOALLOC_MAX_VOXELS voxels return RECON_ERR_UNSUPPORTED;
+ *  - overlapping calls on one device (other streams or host threads) share
+ *    the scratch and corrupt each other; calls in one stream are safe;
+ *  - the first call on a device looks up the scratch address: make it before
+ *    capturing a stream into a CUDA graph.
+ * Uses the current device; asynchronous on `stream`. */
+#define RECON_NOALLOC_MAX_VOXELS 2097152
+recon_status_t recon_compat_bp_view_noalloc(const recon_geometry_t* geom, const float* d_img,
+                                            float angle_deg, float* d_vol, void* stream);
+
 /* ---- file-driven drivers (the reference's siddon_recon entry points) ------ */
 
 /* siddon_recon::a0_RECON_MLEM(folder, cfg) (hf_siddon_recon.hpp:91-108):

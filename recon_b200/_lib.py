@@ -23,6 +23,7 @@ SUM_KAHAN, SUM_PLAIN = 0, 1
 SINO_F32, SINO_BF16 = 0, 1
 BP_SIDDON, BP_VOXEL = 0, 1
 VOXEL_REFERENCE, VOXEL_GEOMETRIC = 0, 1
+NOALLOC_MAX_VOXELS = 2097152  # RECON_NOALLOC_MAX_VOXELS
 
 
 class ReconError(RuntimeError):
@@ -120,6 +121,7 @@ def lib() -> C.CDLL:
         "recon_batch_create": (st, [C.POINTER(Geometry), C.c_int, C.POINTER(Options), C.POINTER(P)]),
         "recon_batch_destroy": (None, [P]),
         "recon_batch_mlem": (st, [P, C.POINTER(P), C.POINTER(P), u, C.c_int, P]),
+        "recon_compat_bp_view_noalloc": (st, [C.POINTER(Geometry), P, f, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name, None)
@@ -141,7 +143,7 @@ def exported_symbols() -> list[str]:
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_set_ones", "recon_divide1", "recon_multiply1",
         "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_view_step_count", "recon_mlem_from_cfg",
         "recon_forward_projection_from_cfg", "recon_backward_projection_from_cfg", "recon_batch_create",
-        "recon_batch_destroy", "recon_batch_mlem",
+        "recon_batch_destroy", "recon_batch_mlem", "recon_compat_bp_view_noalloc",
     ]
 
 

@@ -284,6 +284,16 @@ class Batch:
         return fs
 
 
+def compat_bp_view_noalloc(cfg: dict, img, angle: float, out):
+    """recon_compat_bp_view_noalloc: COMPAT back projection of one view into
+    `out` on the current CUDA device, with no device allocation by the library
+    (at most L.NOALLOC_MAX_VOXELS voxels; overlapping calls on one device
+    share its scratch and must not run concurrently)."""
+    g = geometry(cfg)
+    check(lib().recon_compat_bp_view_noalloc(C.byref(g), _ptr(img), float(angle), _ptr(out), _stream()))
+    return out
+
+
 def mlem_from_cfg(folder: str, cfg: str, options: Options | None = None) -> None:
     """siddon_recon::a0_RECON_MLEM(folder, cfg) (hf_siddon_recon.hpp:91-108)."""
     o = (options or Options()).c()

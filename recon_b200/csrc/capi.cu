@@ -519,3 +519,26 @@ recon_status_t recon_compat_trace(recon_plan_t P, float angle, int nrays, const 
 }
 
 }  // extern "C"
+
+namespace rb {
+
+// Host-side description of a COMPAT geometry in a Plan that owns no device
+// memory (sizes, rotation matrix and the CompatGeom kernel parameters), for
+// callers that point its device fields at buffers of their own.
+recon_status_t describe_compat_geometry(const recon_geometry_t& g, Plan& P)
+{
+    recon_options_t o;
+    recon_default_options(&o);
+    o.arith = RECON_ARITH_COMPAT;
+    RB_CHECK(validate(g, o));
+    P.geom = g;
+    P.opt = o;
+    P.npix = (size_t)g.det.NumAxPixels * g.det.NumTAxPixels;
+    P.nvox = (size_t)g.vox.Xdim * g.vox.Ydim * g.vox.Zdim;
+    P.nviews = 0;
+    host_rotation_matrix(g.cal.xangle, g.cal.yangle, g.cal.zangle, P.RM);
+    fill_geoms(P);
+    return RECON_OK;
+}
+
+}  // namespace rb

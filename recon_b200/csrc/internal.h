@@ -167,6 +167,7 @@ recon_status_t compat_fp_ratio_all(Plan& P, const float* vol, const float* g, fl
 void release_plan_textures(const Plan* P);
 recon_status_t ensure_mlem_buffers(Plan& P);
 recon_status_t compute_sensitivity(Plan& P, float* sens, cudaStream_t s);
+recon_status_t describe_compat_geometry(const recon_geometry_t& g, Plan& P);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);
 recon_status_t launch_update(float* f, const float* ht, const float* sens, size_t n, bool fast_div,
