@@ -1,6 +1,7 @@
 // batch.cu -- many independent MLEM reconstructions per launch.
 //
-// Every iteration of all problems is two persistent kernels: the forward
+// Every iteration of all problems is two persistent kernels (after a
+// transpose of every image, which the forward walk reads for some views): the forward
 // projection with the ratio fused in, over 32x4-ray tiles of every view of
 // every problem, and the gather back projection with the update fused in,
 // over (32x4 column block, z-chunk) tiles of every problem.  CTAs pull tile
@@ -35,6 +36,7 @@ struct BatchProb {
     float* ratio;
     const float* g;
     float* f;
+    float* f_t;  // xy-transposed copy of f, made before each forward projection
     unsigned nviews;
     unsigned fp_tx, fp_ty;
     unsigned bp_bx, bp_by, bp_bz;
@@ -83,11 +85,40 @@ __global__ void __launch_bounds__(128) fp_kernel(const BatchProb* __restrict__ p
         const int2 K = __ldg(B.kxy + (size_t)view * G.Nu + u);
         const ZParam Z = B.zp[v];
         const float w = __ldg(B.w + pix);
-        const float hf = w * exact::fp_ray_sum<KAHAN>(G, T, K, Z, B.f);
+        const exact::VolView V = exact::vol_view_for(__ldg(B.cs + view), B.f, B.f_t, G.X, G.Y);
+        const float hf = w * exact::fp_ray_sum<KAHAN>(G, T, K, Z, V);
         const size_t n = (size_t)view * G.Nu * G.Nv + pix;
         const float gv = __ldg(B.g + n);
         const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
         B.ratio[n] = ratio * w;
+    }
+}
+
+// f -> f_t of every problem, 32x32 tiles (one z slice each) spread over a
+// grid-stride loop; prefix[p] counts the tiles of problems before p.
+__global__ void __launch_bounds__(256) transpose_kernel(const BatchProb* __restrict__ probs,
+                                                         const unsigned long long* __restrict__ prefix, int nprob)
+{
+    __shared__ float tile[32][33];
+    const unsigned long long total = prefix[nprob];
+    for (unsigned long long t = blockIdx.x; t < total; t += gridDim.x) {
+        const int p = find_problem(prefix, nprob, t);
+        const BatchProb& B = probs[p];
+        const int X = B.G.X, Y = B.G.Y;
+        const unsigned tx = (unsigned)(X + 31) / 32, ty = (unsigned)(Y + 31) / 32;
+        const unsigned long long local = t - prefix[p];
+        const int x0 = (int)(local % tx) * 32, y0 = (int)((local / tx) % ty) * 32;
+        const size_t slab = (size_t)X * Y * (size_t)(local / ((unsigned long long)tx * ty));
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int x = x0 + threadIdx.x, y = y0 + r;
+            if (x < X && y < Y) tile[r][threadIdx.x] = B.f[slab + (size_t)y * X + x];
+        }
+        __syncthreads();
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int y = y0 + threadIdx.x, x = x0 + r;
+            if (x < X && y < Y) B.f_t[slab + (size_t)x * Y + y] = tile[threadIdx.x][r];
+        }
+        __syncthreads();
     }
 }
 
@@ -161,6 +192,8 @@ struct recon_batch {
     std::vector<BatchProb> host;
     BatchProb* d_probs = nullptr;
     unsigned long long* d_fp_prefix = nullptr;
+    unsigned long long* d_tr_prefix = nullptr;  // transpose tiles
+    int sm_count = 148;
     unsigned long long* d_bp_prefix[2] = {nullptr, nullptr};  // per zc candidate
     int* d_perm[2] = {nullptr, nullptr};
     unsigned long long* d_counters = nullptr;
@@ -178,6 +211,7 @@ struct recon_batch {
         if (cap_stream) cudaStreamDestroy(cap_stream);
         cudaFree(d_probs);
         cudaFree(d_fp_prefix);
+        cudaFree(d_tr_prefix);
         for (int k = 0; k < 2; ++k) {
             cudaFree(d_bp_prefix[k]);
             cudaFree(d_perm[k]);
@@ -234,6 +268,8 @@ recon_status_t launch_iteration(recon_batch& b, const BatchChoice& c, cudaStream
     const int n = (int)b.host.size();
     const int zci = (c.zc == 16) ? 0 : 1;
     RB_CUDA(cudaMemsetAsync(b.d_counters, 0, 2 * sizeof(unsigned long long), s));
+    batch::transpose_kernel<<<b.sm_count * 8, dim3(32, 8), 0, s>>>(b.d_probs, b.d_tr_prefix, n);
+    RB_CUDA(cudaGetLastError());
     if (b.kahan)
         batch::fp_kernel<true><<<c.fp_ctas, dim3(32, 4), 0, s>>>(b.d_probs, b.d_fp_prefix, n, b.d_counters);
     else
@@ -398,6 +434,7 @@ recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const re
         h.w = P.d_w;
         h.sens = P.d_sens;
         h.ratio = static_cast<float*>(P.d_ratio);
+        h.f_t = P.d_vol_t;
         h.nviews = P.nviews;
         h.fp_tx = (P.eg.Nu + 31) / 32;
         h.fp_ty = (P.eg.Nv + 3) / 4;
@@ -417,6 +454,14 @@ recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const re
         fp_prefix[p + 1] = fp_prefix[p] + (unsigned long long)b->host[p].nviews * b->host[p].fp_tx * b->host[p].fp_ty;
     RB_CUDA(cudaMalloc(&b->d_fp_prefix, (n + 1) * sizeof(unsigned long long)));
     RB_CUDA(cudaMemcpy(b->d_fp_prefix, fp_prefix.data(), (n + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    std::vector<unsigned long long> tr_prefix(n + 1, 0);
+    for (int p = 0; p < n; ++p) {
+        const ExactGeom& G = b->host[p].G;
+        tr_prefix[p + 1] = tr_prefix[p] + (unsigned long long)((G.X + 31) / 32) * ((G.Y + 31) / 32) * G.Z;
+    }
+    RB_CUDA(cudaMalloc(&b->d_tr_prefix, (n + 1) * sizeof(unsigned long long)));
+    RB_CUDA(cudaMemcpy(b->d_tr_prefix, tr_prefix.data(), (n + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    RB_CUDA(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device));
     for (int zci = 0; zci < 2; ++zci) RB_CHECK(build_order(*b, zci));
     RB_CUDA(cudaMalloc(&b->d_probs, n * sizeof(BatchProb)));
     RB_CUDA(cudaMalloc(&b->d_counters, 2 * sizeof(unsigned long long)));

@@ -265,6 +265,7 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_cs, nv1, "view trig"));
             RB_CHECK(P->alloc(&P->d_zp, geom->det.NumTAxPixels, "ray table z"));
             RB_CHECK(P->alloc(&P->d_w, P->npix, "ray weights"));
+            RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
             RB_CHECK(build_exact_tables(*P, 0));
         } else {
             RB_CHECK(P->alloc(&P->d_maxabs, nv1, "maxabs"));

@@ -117,14 +117,16 @@ __global__ void w_table_kernel(GeomD G, float* __restrict__ w)
 template <bool KAHAN, int MODE, class GT, class OT>
 __global__ void __launch_bounds__(128) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                   const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
-                                                  const float* __restrict__ wtab, unsigned view0,
-                                                  const float* __restrict__ vol, const GT* __restrict__ g,
+                                                  const float* __restrict__ wtab, const float2* __restrict__ cs,
+                                                  unsigned view0, const float* __restrict__ vol,
+                                                  const float* __restrict__ vol_t, const GT* __restrict__ g,
                                                   OT* __restrict__ out)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int v = blockIdx.y * blockDim.y + threadIdx.y;
     const unsigned view = view0 + blockIdx.z;
     if (u >= G.Nu || v >= G.Nv) return;
+    const VolView V = vol_view_for(__ldg(cs + view), vol, vol_t, G.X, G.Y);
     const size_t pix = (size_t)u + (size_t)v * G.Nu;
     const size_t n = (size_t)blockIdx.z * G.Nu * G.Nv + pix;
     const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
@@ -132,7 +134,7 @@ __global__ void __launch_bounds__(128) fp_kernel(ExactGeom G, const float4* __re
     const ZParam Z = zp[v];
     const float w = __ldg(wtab + pix);
 
-    const float acc = fp_ray_sum<KAHAN>(G, T, K, Z, vol);
+    const float acc = fp_ray_sum<KAHAN>(G, T, K, Z, V);
     const float hf = w * acc;
     if (MODE == 0) {
         store_val<OT>(out + n, hf);
@@ -250,6 +252,53 @@ recon_status_t exact_view_table(Plan& P, float angle, cudaStream_t s)
 static dim3 fp_block() { return dim3(32, 4, 1); }
 static dim3 fp_grid(const Plan& P, unsigned views) { return dim3((P.eg.Nu + 31) / 32, (P.eg.Nv + 3) / 4, views); }
 
+namespace exact {
+// f[z][y][x] -> ft[z][x][y], 32x32 tiles through shared memory
+__global__ void __launch_bounds__(256) transpose_xy_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                           int X, int Y)
+{
+    __shared__ float tile[32][33];
+    const size_t slab = (size_t)X * Y * blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int x = x0 + threadIdx.x, y = y0 + r;
+        if (x < X && y < Y) tile[r][threadIdx.x] = in[slab + (size_t)y * X + x];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int y = y0 + threadIdx.x, x = x0 + r;
+        if (x < X && y < Y) out[slab + (size_t)x * Y + y] = tile[threadIdx.x][r];
+    }
+}
+}  // namespace exact
+
+recon_status_t exact_transpose(const float* vol, float* vol_t, int X, int Y, int Z, cudaStream_t s)
+{
+    exact::transpose_xy_kernel<<<dim3((X + 31) / 32, (Y + 31) / 32, Z), dim3(32, 8), 0, s>>>(vol, vol_t, X, Y);
+    RB_CUDA(cudaGetLastError());
+    return RECON_OK;
+}
+
+// Forward projection of views [first, first+count) (table slots), reading the
+// volume in the layout that suits each view (the transposed copy is made
+// here, once per call).
+template <int MODE, class GT, class OT>
+static recon_status_t launch_fp(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g, OT* out,
+                                cudaStream_t s)
+{
+    if (count == 0) return RECON_OK;
+    RB_CHECK(exact_transpose(vol, P.d_vol_t, P.eg.X, P.eg.Y, P.eg.Z, s));
+    const dim3 grid = fp_grid(P, count), blk = fp_block();
+    if (P.opt.sum == RECON_SUM_KAHAN)
+        exact::fp_kernel<true, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
+                                                                  first, vol, P.d_vol_t, g, out);
+    else
+        exact::fp_kernel<false, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
+                                                                   first, vol, P.d_vol_t, g, out);
+    RB_CUDA(cudaGetLastError());
+    return RECON_OK;
+}
+
 recon_status_t exact_fp(Plan& P, const float* vol, unsigned first, unsigned count, bool scratch_slot, float* out,
                         cudaStream_t s)
 {
@@ -257,47 +306,17 @@ recon_status_t exact_fp(Plan& P, const float* vol, unsigned first, unsigned coun
         first = P.nviews;
         count = 1;
     }
-    if (count == 0) return RECON_OK;
-    if (P.opt.sum == RECON_SUM_KAHAN)
-        exact::fp_kernel<true, 0, float, float><<<fp_grid(P, count), fp_block(), 0, s>>>(
-            P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, first, vol, nullptr, out);
-    else
-        exact::fp_kernel<false, 0, float, float><<<fp_grid(P, count), fp_block(), 0, s>>>(
-            P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, first, vol, nullptr, out);
-    RB_CUDA(cudaGetLastError());
-    return RECON_OK;
+    return launch_fp<0, float, float>(P, vol, first, count, nullptr, out, s);
 }
 
 recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ratio, cudaStream_t s,
                               unsigned first, unsigned count)
 {
-    if (count == 0) return RECON_OK;
-    const bool kahan = P.opt.sum == RECON_SUM_KAHAN;
-    const bool bf16 = P.opt.sino == RECON_SINO_BF16;
-    const dim3 grid = fp_grid(P, count), blk = fp_block();
     const size_t off = (size_t)first * P.npix;
     using bf = __nv_bfloat16;
-    if (bf16) {
-        const bf* gb = (const bf*)g + off;
-        bf* rb = (bf*)ratio + off;
-        if (kahan)
-            exact::fp_kernel<true, 1, bf, bf><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, first, vol,
-                                                                   gb, rb);
-        else
-            exact::fp_kernel<false, 1, bf, bf><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, first, vol,
-                                                                    gb, rb);
-    } else {
-        const float* gf = (const float*)g + off;
-        float* rf = (float*)ratio + off;
-        if (kahan)
-            exact::fp_kernel<true, 1, float, float><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, first,
-                                                                         vol, gf, rf);
-        else
-            exact::fp_kernel<false, 1, float, float><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w,
-                                                                          first, vol, gf, rf);
-    }
-    RB_CUDA(cudaGetLastError());
-    return RECON_OK;
+    if (P.opt.sino == RECON_SINO_BF16)
+        return launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + off, s);
+    return launch_fp<1, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + off, s);
 }
 
 // Number of (ray, voxel) pairs with positive length: the forward walk with
@@ -371,14 +390,7 @@ recon_status_t exact_count(Plan& P, unsigned long long* out)
 
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s)
 {
-    if (P.opt.sum == RECON_SUM_KAHAN)
-        exact::fp_kernel<true, 2, float, float><<<fp_grid(P, P.nviews), fp_block(), 0, s>>>(
-            P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, 0u, vol, g, ratio);
-    else
-        exact::fp_kernel<false, 2, float, float><<<fp_grid(P, P.nviews), fp_block(), 0, s>>>(
-            P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, 0u, vol, g, ratio);
-    RB_CUDA(cudaGetLastError());
-    return RECON_OK;
+    return launch_fp<2, float, float>(P, vol, 0u, P.nviews, g, ratio, s);
 }
 
 template <int ZC, int MODE, bool WEIGHTED, class ST>

@@ -53,13 +53,30 @@ __device__ __forceinline__ void store_val<__nv_bfloat16>(__nv_bfloat16* p, float
 
 // ---- forward projection --------------------------------------------------------------------
 
+// The volume as the forward walk reads it: voxel (x, y, z) at
+// base[x*ux + y*uy + z*X*Y].  ux = 1, uy = X is the image layout; ux = Y,
+// uy = 1 is its xy-transposed copy, read for views whose detector rows run
+// mostly along y (|sin| > |cos|), so that the 32 rays of a warp (adjacent
+// detector columns) read adjacent addresses in either case.
+struct VolView {
+    const float* __restrict__ base;
+    int ux, uy;
+};
+
+__device__ __forceinline__ VolView vol_view_for(const float2 cs, const float* vol, const float* vol_t, int X, int Y)
+{
+    if (vol_t && fabsf(cs.y) > fabsf(cs.x)) return VolView{vol_t, Y, 1};
+    return VolView{vol, 1, X};
+}
+
 // Sum over the voxels the ray crosses of (t_exit - t_entry) * f[voxel] (the
 // projection divided by w): entry and exit voxels located per ray, the step
 // count known before the walk, one axis advanced per step.
 template <bool KAHAN>
 __device__ __forceinline__ float fp_ray_sum(const ExactGeom& G, const float4 T, const int2 K, const ZParam Z,
-                                            const float* __restrict__ vol)
+                                            const VolView V)
 {
+    const float* __restrict__ vol = V.base;
     // entry / exit planes of the volume
     float x0 = plane_t(0, T.x, T.y, K.x), x1 = plane_t(G.X, T.x, T.y, K.x);
     float y0 = plane_t(0, T.z, T.w, K.y), y1 = plane_t(G.Y, T.z, T.w, K.y);
@@ -80,9 +97,9 @@ __device__ __forceinline__ float fp_ray_sum(const ExactGeom& G, const float4 T, 
         float kz = (float)((dz > 0 ? iz + 1 : iz) - Z.kc);
         float tx = fmaf(kx, T.x, T.y), ty = fmaf(ky, T.z, T.w), tz = fmaf(kz, Z.S, Z.O);
         const float fdx = (float)dx, fdy = (float)dy, fdz = (float)dz;
-        const int sx = dx, sy = dy * G.X, sz = dz * G.X * G.Y;
+        const int sx = dx * V.ux, sy = dy * V.uy, sz = dz * G.X * G.Y;
         const unsigned vmax = (unsigned)(G.X * G.Y * G.Z - 1);
-        int idx = ix + iy * G.X + iz * G.X * G.Y;
+        int idx = ix * V.ux + iy * V.uy + iz * G.X * G.Y;
         float cur = t_in, comp = 0.0f;
 #pragma unroll 2
         for (int s = 0; s < nsteps; ++s) {

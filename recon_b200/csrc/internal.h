@@ -94,6 +94,7 @@ struct Plan {
     float2* d_cs = nullptr;    // [view] {cos, sin} of the view angle
     ZParam* d_zp = nullptr;    // [v]
     float* d_w = nullptr;      // [v][u] |p2-p1| / R
+    float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y]
     // scratch view slot for arbitrary-angle single-view calls (index nviews)
     float* d_angles = nullptr;    // [view] (float)n*DeltaAng, + 1 scratch slot
     // COMPAT tables
@@ -168,6 +169,7 @@ void release_plan_textures(const Plan* P);
 recon_status_t ensure_mlem_buffers(Plan& P);
 recon_status_t compute_sensitivity(Plan& P, float* sens, cudaStream_t s);
 recon_status_t describe_compat_geometry(const recon_geometry_t& g, Plan& P);
+recon_status_t exact_transpose(const float* vol, float* vol_t, int X, int Y, int Z, cudaStream_t s);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);
 recon_status_t launch_update(float* f, const float* ht, const float* sens, size_t n, bool fast_div,
