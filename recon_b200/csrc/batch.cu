@@ -1,19 +1,26 @@
 // batch.cu -- many independent MLEM reconstructions per launch.
 //
-// Every iteration of all problems is two persistent kernels (after a
-// transpose of every image, which the forward walk reads for some views): the forward
-// projection with the ratio fused in, over 32x4-ray tiles of every view of
-// every problem, and the gather back projection with the update fused in,
-// over (32x4 column block, z-chunk) tiles of every problem.  CTAs pull tile
-// indices from an atomic counter; back-projection tiles are ordered by
-// decreasing cost (views x rows per chunk), longest first, so the last wave
-// is short.  The per-ray and per-column work is the same device code as the
-// single-problem kernels (exact_device.cuh), so each problem's result is
-// bit-identical to recon_mlem on its own plan.  One iteration (counter reset
-// + two launches) is captured once in a CUDA graph and replayed.  The z-chunk
-// size and the number of resident CTAs are picked by timing graph replays on
-// the first call (cached per shape class for the process).
+// One iteration of all problems is four kernels, captured once in a CUDA
+// graph and replayed:
+//  1. a transpose of every image (the forward walk reads the xy-transposed
+//     copy for views whose detector rows run along y), which also clears
+//     every problem's max-|ratio| slot;
+//  2. the forward projection with the ratio fused in, a persistent kernel
+//     over the 32x4-ray blocks of every problem that can cross its volume
+//     (the plans' culled tile lists), recording each problem's max |ratio|;
+//  3. the back projection of the ratios, a persistent kernel over the same
+//     ray tiles, adding to each problem's fixed-point accumulators;
+//  4. the update f <- f * Ht / sens of every problem, which also clears the
+//     accumulators.
+// CTAs of 2 and 3 pull tile indices from atomic counters; problems are queued
+// largest first, so the last tiles are small.  The per-ray work is the same
+// device code as the single-problem kernels (exact_device.cuh) and the back
+// projection sums exactly, so each problem's image is bit-identical to
+// recon_mlem on its own plan whatever the tile order.  The number of resident
+// CTAs of kernels 2 and 3 is picked by timing graph replays on the first call
+// (cached per set of shapes for the process).
 #include <algorithm>
+#include <climits>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -36,10 +43,15 @@ struct BatchProb {
     float* ratio;
     const float* g;
     float* f;
-    float* f_t;  // xy-transposed copy of f, made before each forward projection
+    float* f_t;                    // xy-transposed copy of f, made before each forward projection
+    unsigned long long* acc;       // back projection accumulators, image layout [nvox]
+    unsigned long long* acc_t;     // and xy-transposed [nvox]
+    unsigned* bpmax;               // max |ratio| of the current iteration (float bits)
+    float max_len;                 // longest segment (fixed-point scale)
+    int count_bits;                // contributions per voxel, as bits (fixed-point scale)
+    const uint2* tiles;            // ray blocks that can cross the volume ({view, tu | tv << 16})
+    unsigned ntiles;
     unsigned nviews;
-    unsigned fp_tx, fp_ty;
-    unsigned bp_bx, bp_by, bp_bz;
 };
 
 namespace batch {
@@ -56,50 +68,15 @@ __device__ __forceinline__ int find_problem(const unsigned long long* prefix, in
     return lo;
 }
 
-template <bool KAHAN>
-__global__ void __launch_bounds__(128) fp_kernel(const BatchProb* __restrict__ probs,
-                                                  const unsigned long long* __restrict__ prefix, int nprob,
-                                                  unsigned long long* __restrict__ counter)
-{
-    __shared__ unsigned long long s_tile;
-    const int tid = threadIdx.x + threadIdx.y * 32;
-    const unsigned long long total = prefix[nprob];
-    for (;;) {
-        if (tid == 0) s_tile = atomicAdd(counter, 1ull);
-        __syncthreads();
-        const unsigned long long t = s_tile;
-        __syncthreads();
-        if (t >= total) return;
-        const int p = find_problem(prefix, nprob, t);
-        const BatchProb& B = probs[p];
-        const ExactGeom G = B.G;
-        const unsigned per_view = B.fp_tx * B.fp_ty;
-        const unsigned long long local = t - prefix[p];
-        const unsigned view = (unsigned)(local / per_view);
-        const unsigned r = (unsigned)(local % per_view);
-        const int u = (int)(r % B.fp_tx) * 32 + threadIdx.x;
-        const int v = (int)(r / B.fp_tx) * 4 + threadIdx.y;
-        if (u >= G.Nu || v >= G.Nv) continue;
-        const size_t pix = (size_t)u + (size_t)v * G.Nu;
-        const float4 T = __ldg(B.txy + (size_t)view * G.Nu + u);
-        const int2 K = __ldg(B.kxy + (size_t)view * G.Nu + u);
-        const ZParam Z = B.zp[v];
-        const float w = __ldg(B.w + pix);
-        const exact::VolView V = exact::vol_view_for(__ldg(B.cs + view), B.f, B.f_t, G.X, G.Y);
-        const float hf = w * exact::fp_ray_sum<KAHAN>(G, T, K, Z, V);
-        const size_t n = (size_t)view * G.Nu * G.Nv + pix;
-        const float gv = __ldg(B.g + n);
-        const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-        B.ratio[n] = ratio * w;
-    }
-}
-
 // f -> f_t of every problem, 32x32 tiles (one z slice each) spread over a
-// grid-stride loop; prefix[p] counts the tiles of problems before p.
+// grid-stride loop; prefix[p] counts the tiles of problems before p.  Block 0
+// also clears every problem's max-|ratio| slot for the forward kernel.
 __global__ void __launch_bounds__(256) transpose_kernel(const BatchProb* __restrict__ probs,
                                                          const unsigned long long* __restrict__ prefix, int nprob)
 {
     __shared__ float tile[32][33];
+    if (blockIdx.x == 0)
+        for (int p = threadIdx.x + threadIdx.y * 32; p < nprob; p += 256) *probs[p].bpmax = 0u;
     const unsigned long long total = prefix[nprob];
     for (unsigned long long t = blockIdx.x; t < total; t += gridDim.x) {
         const int p = find_problem(prefix, nprob, t);
@@ -122,61 +99,117 @@ __global__ void __launch_bounds__(256) transpose_kernel(const BatchProb* __restr
     }
 }
 
-template <int ZC>
+// Ray tile t of the queue: problem perm[q], view and the 32x4 block of rays.
+struct RayTile {
+    int p, u, v;
+    unsigned view;
+};
+
+__device__ __forceinline__ RayTile ray_tile(const BatchProb* probs, const unsigned long long* prefix,
+                                            const int* perm, int nprob, unsigned long long t)
+{
+    const int q = find_problem(prefix, nprob, t);
+    const int p = perm[q];
+    const uint2 tile = probs[p].tiles[t - prefix[q]];
+    return RayTile{p, (int)(tile.y & 0xffffu) * 32 + (int)threadIdx.x, (int)(tile.y >> 16) * 4 + (int)threadIdx.y,
+                   tile.x};
+}
+
+// Next tile index for the whole CTA (one atomic per tile).
+__device__ __forceinline__ unsigned long long next_tile(unsigned long long* counter, unsigned long long* s_tile,
+                                                        int tid)
+{
+    if (tid == 0) *s_tile = atomicAdd(counter, 1ull);
+    __syncthreads();
+    const unsigned long long t = *s_tile;
+    __syncthreads();
+    return t;
+}
+
+template <bool KAHAN>
+__global__ void __launch_bounds__(128) fp_kernel(const BatchProb* __restrict__ probs,
+                                                  const unsigned long long* __restrict__ prefix,
+                                                  const int* __restrict__ perm, int nprob,
+                                                  unsigned long long* __restrict__ counter)
+{
+    __shared__ unsigned long long s_tile;
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const unsigned long long total = prefix[nprob];
+    for (;;) {
+        const unsigned long long t = next_tile(counter, &s_tile, tid);
+        if (t >= total) return;
+        const RayTile R = ray_tile(probs, prefix, perm, nprob, t);
+        const BatchProb& B = probs[R.p];
+        const ExactGeom G = B.G;
+        unsigned m = 0;
+        if (R.u < G.Nu && R.v < G.Nv) {
+            const size_t pix = (size_t)R.u + (size_t)R.v * G.Nu;
+            const float4 T = __ldg(B.txy + (size_t)R.view * G.Nu + R.u);
+            const int2 K = __ldg(B.kxy + (size_t)R.view * G.Nu + R.u);
+            const ZParam Z = B.zp[R.v];
+            const float w = __ldg(B.w + pix);
+            const exact::VolView V = exact::vol_view_for(__ldg(B.cs + R.view), B.f, B.f_t, G.X, G.Y);
+            const float hf = w * exact::fp_ray_sum<KAHAN>(G, T, K, Z, V);
+            const size_t n = (size_t)R.view * G.Nu * G.Nv + pix;
+            const float gv = __ldg(B.g + n);
+            const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
+            const float out = ratio * w;
+            B.ratio[n] = out;
+            m = __float_as_uint(fabsf(out));
+        }
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0 && m) atomicMax(B.bpmax, m);
+    }
+}
+
 __global__ void __launch_bounds__(128) bp_kernel(const BatchProb* __restrict__ probs,
                                                   const unsigned long long* __restrict__ prefix,
                                                   const int* __restrict__ perm, int nprob,
                                                   unsigned long long* __restrict__ counter)
 {
-    extern __shared__ float smem[];
-    float* acc = smem;
-    float4* szb = reinterpret_cast<float4*>(smem + ZC * 128);
     __shared__ unsigned long long s_tile;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const unsigned long long total = prefix[nprob];
     for (;;) {
-        if (tid == 0) s_tile = atomicAdd(counter, 1ull);
-        __syncthreads();
-        const unsigned long long t = s_tile;
+        const unsigned long long t = next_tile(counter, &s_tile, tid);
         if (t >= total) return;
-        const int q = find_problem(prefix, nprob, t);
-        const BatchProb& B = probs[perm[q]];
+        const RayTile R = ray_tile(probs, prefix, perm, nprob, t);
+        const BatchProb& B = probs[R.p];
         const ExactGeom G = B.G;
-        const unsigned long long local = t - prefix[q];
-        const unsigned bx = (unsigned)(local % B.bp_bx);
-        const unsigned by = (unsigned)((local / B.bp_bx) % B.bp_by);
-        const unsigned bz = (unsigned)(local / ((unsigned long long)B.bp_bx * B.bp_by));
-        for (int z = tid; z < G.Nv; z += 128) {
-            const ZParam zz = B.zp[z];
-            const bool pos = zz.S > 0.0f;
-            szb[z] = make_float4(fabsf(zz.S), pos ? zz.O : -zz.O, (float)zz.kc, pos ? 1.0f : -1.0f);
-        }
-#pragma unroll
-        for (int k = 0; k < ZC; ++k) acc[k * 128 + tid] = 0.0f;
-        __syncthreads();
-        const int i = (int)bx * 32 + threadIdx.x;
-        const int j = (int)by * 4 + threadIdx.y;
-        const int k0 = (int)bz * ZC;
-        const int k1 = min(k0 + ZC, G.Z);
-        if (i < G.X && j < G.Y) {
-            exact::bp_gather_column<ZC, 2, false, float>(G, B.txy, B.kxy, B.cs, B.w, 0u, B.nviews, B.ratio, szb,
-                                                         acc, tid, i, j, k0, k1);
-            for (int k = k0; k < k1; ++k) {
-                const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)k * G.X * G.Y;
-                const float ht = acc[(k - k0) * 128 + tid];
-                const float s = B.sens[vox];
-                const float f = B.f[vox];
-                B.f[vox] = (s != 0.0f) ? __fdiv_rn(__fmul_rn(f, ht), s) : 0.0f;
-            }
-        }
-        __syncthreads();
+        if (R.u >= G.Nu || R.v >= G.Nv) continue;
+        const int F = exact::fix_exponent(*B.bpmax, B.max_len, B.count_bits);
+        if (F == INT_MIN) continue;
+        const float val = B.ratio[(size_t)R.view * G.Nu * G.Nv + (size_t)R.u + (size_t)R.v * G.Nu];
+        if (val == 0.0f) continue;
+        const float2 C = __ldg(B.cs + R.view);
+        exact::bp_ray_slab(G, __ldg(B.txy + (size_t)R.view * G.Nu + R.u), __ldg(B.kxy + (size_t)R.view * G.Nu + R.u),
+                           B.zp[R.v], 0, G.Z, val * ldexpf(1.0f, F), fabsf(C.y) > fabsf(C.x), B.acc, B.acc_t);
+    }
+}
+
+// f <- (sens != 0) ? f * Ht / sens : 0 for every voxel of every problem;
+// prefix[p] counts the voxels of problems before p.
+__global__ void __launch_bounds__(256) update_kernel(const BatchProb* __restrict__ probs,
+                                                      const unsigned long long* __restrict__ prefix, int nprob)
+{
+    const unsigned long long total = prefix[nprob];
+    for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < total;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        const int p = find_problem(prefix, nprob, t);
+        const BatchProb& B = probs[p];
+        const ExactGeom G = B.G;
+        const size_t i = (size_t)(t - prefix[p]);
+        const int x = (int)(i % G.X), y = (int)((i / G.X) % G.Y), z = (int)(i / ((size_t)G.X * G.Y));
+        const int F = exact::fix_exponent(*B.bpmax, B.max_len, B.count_bits);
+        const float ht = exact::bp_slab_value(G, x, y, z, F, B.acc, B.acc_t);
+        const float sv = B.sens[i];
+        B.f[i] = (sv != 0.0f) ? __fdiv_rn(__fmul_rn(B.f[i], ht), sv) : 0.0f;
     }
 }
 
 }  // namespace batch
 
 struct BatchChoice {
-    int zc = 32;
     int fp_ctas = 0;
     int bp_ctas = 0;
 };
@@ -191,31 +224,29 @@ struct recon_batch {
     bool kahan = true;
     std::vector<BatchProb> host;
     BatchProb* d_probs = nullptr;
-    unsigned long long* d_fp_prefix = nullptr;
-    unsigned long long* d_tr_prefix = nullptr;  // transpose tiles
-    int sm_count = 148;
-    unsigned long long* d_bp_prefix[2] = {nullptr, nullptr};  // per zc candidate
-    int* d_perm[2] = {nullptr, nullptr};
+    unsigned long long* d_ray_prefix = nullptr;  // ray tiles, problems in queue order
+    int* d_perm = nullptr;                       // queue order -> problem
+    unsigned long long* d_tr_prefix = nullptr;   // transpose tiles
+    unsigned long long* d_vox_prefix = nullptr;  // voxels
+    unsigned long long* d_acc = nullptr;         // all problems' accumulators
     unsigned long long* d_counters = nullptr;
-    size_t max_nv = 0;
+    int sm_count = 148;
     std::string key;
     BatchChoice choice;
     bool tuned = false;
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t exec = nullptr;
-    const float* const* graph_g = nullptr;
 
     ~recon_batch()
     {
         if (exec) cudaGraphExecDestroy(exec);
         if (cap_stream) cudaStreamDestroy(cap_stream);
         cudaFree(d_probs);
-        cudaFree(d_fp_prefix);
+        cudaFree(d_ray_prefix);
+        cudaFree(d_perm);
         cudaFree(d_tr_prefix);
-        for (int k = 0; k < 2; ++k) {
-            cudaFree(d_bp_prefix[k]);
-            cudaFree(d_perm[k]);
-        }
+        cudaFree(d_vox_prefix);
+        cudaFree(d_acc);
         cudaFree(d_counters);
         for (auto p : plans) recon_plan_destroy(p);
     }
@@ -223,78 +254,41 @@ struct recon_batch {
 
 namespace {
 
-const int kZC[2] = {16, 32};
-
 std::map<std::string, BatchChoice>& tune_cache()
 {
     static std::map<std::string, BatchChoice> c;
     return c;
 }
 
-recon_status_t build_order(recon_batch& b, int zci)
+recon_status_t upload(unsigned long long** d, const std::vector<unsigned long long>& h)
 {
-    const int ZC = kZC[zci];
-    const int n = (int)b.host.size();
-    std::vector<double> cost(n);
-    std::vector<unsigned long long> tiles(n);
-    for (int p = 0; p < n; ++p) {
-        const ExactGeom& G = b.host[p].G;
-        const unsigned bx = (G.X + 31) / 32, by = (G.Y + 3) / 4, bz = (G.Z + ZC - 1) / ZC;
-        tiles[p] = (unsigned long long)bx * by * bz;
-        // per tile: views x detector rows a chunk of ZC voxels spans
-        cost[p] = (double)b.host[p].nviews * std::min(ZC, G.Z) * (double)G.Nv / G.Z;
-    }
-    std::vector<int> perm(n);
-    std::iota(perm.begin(), perm.end(), 0);
-    std::stable_sort(perm.begin(), perm.end(), [&](int a, int c) { return cost[a] > cost[c]; });
-    std::vector<unsigned long long> prefix(n + 1, 0);
-    for (int q = 0; q < n; ++q) prefix[q + 1] = prefix[q] + tiles[perm[q]];
-    RB_CUDA(cudaMalloc(&b.d_bp_prefix[zci], (n + 1) * sizeof(unsigned long long)));
-    RB_CUDA(cudaMalloc(&b.d_perm[zci], n * sizeof(int)));
-    RB_CUDA(cudaMemcpy(b.d_bp_prefix[zci], prefix.data(), (n + 1) * sizeof(unsigned long long),
-                       cudaMemcpyHostToDevice));
-    RB_CUDA(cudaMemcpy(b.d_perm[zci], perm.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    RB_CUDA(cudaMalloc(d, h.size() * sizeof(unsigned long long)));
+    RB_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
     return RECON_OK;
-}
-
-template <int ZC>
-size_t bp_smem(const recon_batch& b)
-{
-    return (size_t)ZC * 128 * sizeof(float) + b.max_nv * sizeof(float4);
 }
 
 recon_status_t launch_iteration(recon_batch& b, const BatchChoice& c, cudaStream_t s)
 {
     const int n = (int)b.host.size();
-    const int zci = (c.zc == 16) ? 0 : 1;
     RB_CUDA(cudaMemsetAsync(b.d_counters, 0, 2 * sizeof(unsigned long long), s));
     batch::transpose_kernel<<<b.sm_count * 8, dim3(32, 8), 0, s>>>(b.d_probs, b.d_tr_prefix, n);
     RB_CUDA(cudaGetLastError());
     if (b.kahan)
-        batch::fp_kernel<true><<<c.fp_ctas, dim3(32, 4), 0, s>>>(b.d_probs, b.d_fp_prefix, n, b.d_counters);
+        batch::fp_kernel<true><<<c.fp_ctas, dim3(32, 4), 0, s>>>(b.d_probs, b.d_ray_prefix, b.d_perm, n,
+                                                                 b.d_counters);
     else
-        batch::fp_kernel<false><<<c.fp_ctas, dim3(32, 4), 0, s>>>(b.d_probs, b.d_fp_prefix, n, b.d_counters);
+        batch::fp_kernel<false><<<c.fp_ctas, dim3(32, 4), 0, s>>>(b.d_probs, b.d_ray_prefix, b.d_perm, n,
+                                                                  b.d_counters);
     RB_CUDA(cudaGetLastError());
-    if (c.zc == 16)
-        batch::bp_kernel<16><<<c.bp_ctas, dim3(32, 4), bp_smem<16>(b), s>>>(b.d_probs, b.d_bp_prefix[zci],
-                                                                            b.d_perm[zci], n, b.d_counters + 1);
-    else
-        batch::bp_kernel<32><<<c.bp_ctas, dim3(32, 4), bp_smem<32>(b), s>>>(b.d_probs, b.d_bp_prefix[zci],
-                                                                            b.d_perm[zci], n, b.d_counters + 1);
+    batch::bp_kernel<<<c.bp_ctas, dim3(32, 4), 0, s>>>(b.d_probs, b.d_ray_prefix, b.d_perm, n, b.d_counters + 1);
+    RB_CUDA(cudaGetLastError());
+    batch::update_kernel<<<b.sm_count * 8, 256, 0, s>>>(b.d_probs, b.d_vox_prefix, n);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
 
 recon_status_t capture(recon_batch& b, const BatchChoice& c)
 {
-    // the dynamic shared memory limit is per kernel, process-wide: set it for
-    // this batch's largest detector before every capture
-    if (c.zc == 16)
-        RB_CUDA(cudaFuncSetAttribute(batch::bp_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)bp_smem<16>(b)));
-    else
-        RB_CUDA(cudaFuncSetAttribute(batch::bp_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)bp_smem<32>(b)));
     if (b.exec) {
         cudaGraphExecDestroy(b.exec);
         b.exec = nullptr;
@@ -314,26 +308,6 @@ recon_status_t capture(recon_batch& b, const BatchChoice& c)
     return RECON_OK;
 }
 
-recon_status_t occupancy(recon_batch& b, int zc, int& fp_ctas, int& bp_ctas)
-{
-    int sms = 148, nfp = 1, nbp = 1;
-    RB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device));
-    if (b.kahan) RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nfp, batch::fp_kernel<true>, 128, 0));
-    else RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nfp, batch::fp_kernel<false>, 128, 0));
-    if (zc == 16) {
-        RB_CUDA(cudaFuncSetAttribute(batch::bp_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)bp_smem<16>(b)));
-        RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp, batch::bp_kernel<16>, 128, bp_smem<16>(b)));
-    } else {
-        RB_CUDA(cudaFuncSetAttribute(batch::bp_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)bp_smem<32>(b)));
-        RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp, batch::bp_kernel<32>, 128, bp_smem<32>(b)));
-    }
-    fp_ctas = sms * std::max(1, nfp);
-    bp_ctas = sms * std::max(1, nbp);
-    return RECON_OK;
-}
-
 // Time graph replays of each candidate on the caller's data, restoring the
 // images afterwards.
 recon_status_t autotune(recon_batch& b, float* const* d_f)
@@ -343,6 +317,15 @@ recon_status_t autotune(recon_batch& b, float* const* d_f)
         b.choice = it->second;
         return capture(b, b.choice);
     }
+    int nfp = 1, nbp = 1;
+    if (b.kahan) RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nfp, batch::fp_kernel<true>, 128, 0));
+    else RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nfp, batch::fp_kernel<false>, 128, 0));
+    RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp, batch::bp_kernel, 128, 0));
+    nfp = std::max(1, nfp);
+    nbp = std::max(1, nbp);
+    std::vector<BatchChoice> cands;
+    for (int fdiv : {1, 2})
+        for (int bdiv : {1, 2}) cands.push_back({b.sm_count * std::max(1, nfp / fdiv), b.sm_count * std::max(1, nbp / bdiv)});
     size_t total = 0;
     for (auto& h : b.host) total += (size_t)h.G.X * h.G.Y * h.G.Z;
     float* save = nullptr;
@@ -352,17 +335,6 @@ recon_status_t autotune(recon_batch& b, float* const* d_f)
         const size_t n = (size_t)b.host[p].G.X * b.host[p].G.Y * b.host[p].G.Z;
         cudaMemcpyAsync(save + off, d_f[p], n * sizeof(float), cudaMemcpyDeviceToDevice, b.cap_stream);
         off += n;
-    }
-    std::vector<BatchChoice> cands;
-    for (int zc : {16, 32}) {
-        int fpc, bpc;
-        recon_status_t st = occupancy(b, zc, fpc, bpc);
-        if (st != RECON_OK) {
-            cudaFree(save);
-            return st;
-        }
-        cands.push_back({zc, fpc, bpc});
-        if (bpc > 148) cands.push_back({zc, fpc, bpc / 2});
     }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -418,6 +390,7 @@ recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const re
     b->device = opt.device;
     b->kahan = (opt.sum == RECON_SUM_KAHAN);
     std::string key = std::to_string(n) + (b->kahan ? "k" : "p");
+    size_t nvox_total = 0;
     for (int p = 0; p < n; ++p) {
         recon_plan_t plan = nullptr;
         RB_CHECK(recon_plan_create(&geoms[p], &opt, &plan));
@@ -435,13 +408,14 @@ recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const re
         h.sens = P.d_sens;
         h.ratio = static_cast<float*>(P.d_ratio);
         h.f_t = P.d_vol_t;
+        h.bpmax = P.d_bpmax;
+        h.max_len = bp_max_len(P);
+        h.count_bits = bp_count_bits(P, P.nviews);
         h.nviews = P.nviews;
-        h.fp_tx = (P.eg.Nu + 31) / 32;
-        h.fp_ty = (P.eg.Nv + 3) / 4;
-        h.bp_bx = (P.eg.X + 31) / 32;
-        h.bp_by = (P.eg.Y + 3) / 4;
-        b->max_nv = std::max(b->max_nv, (size_t)P.eg.Nv);
+        h.tiles = P.fp_tiles.d;
+        h.ntiles = P.fp_tiles.prefix.empty() ? 0u : P.fp_tiles.prefix.back();
         b->host.push_back(h);
+        nvox_total += P.nvox;
         const recon_geometry_t& g = geoms[p];
         key += "|" + std::to_string(g.vox.Xdim) + "x" + std::to_string(g.vox.Ydim) + "x" + std::to_string(g.vox.Zdim) +
                "/" + std::to_string(g.scan.NumProj) + "/" + std::to_string(g.det.NumAxPixels) + "x" +
@@ -449,20 +423,41 @@ recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const re
     }
     b->key = key;
     RB_CUDA(cudaSetDevice(b->device));
-    std::vector<unsigned long long> fp_prefix(n + 1, 0);
-    for (int p = 0; p < n; ++p)
-        fp_prefix[p + 1] = fp_prefix[p] + (unsigned long long)b->host[p].nviews * b->host[p].fp_tx * b->host[p].fp_ty;
-    RB_CUDA(cudaMalloc(&b->d_fp_prefix, (n + 1) * sizeof(unsigned long long)));
-    RB_CUDA(cudaMemcpy(b->d_fp_prefix, fp_prefix.data(), (n + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
-    std::vector<unsigned long long> tr_prefix(n + 1, 0);
-    for (int p = 0; p < n; ++p) {
-        const ExactGeom& G = b->host[p].G;
-        tr_prefix[p + 1] = tr_prefix[p] + (unsigned long long)((G.X + 31) / 32) * ((G.Y + 31) / 32) * G.Z;
-    }
-    RB_CUDA(cudaMalloc(&b->d_tr_prefix, (n + 1) * sizeof(unsigned long long)));
-    RB_CUDA(cudaMemcpy(b->d_tr_prefix, tr_prefix.data(), (n + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
     RB_CUDA(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device));
-    for (int zci = 0; zci < 2; ++zci) RB_CHECK(build_order(*b, zci));
+    // accumulators: two per problem, cleared once here and by every update
+    RB_CUDA(cudaMalloc(&b->d_acc, 2 * nvox_total * sizeof(unsigned long long)));
+    RB_CUDA(cudaMemset(b->d_acc, 0, 2 * nvox_total * sizeof(unsigned long long)));
+    size_t off = 0;
+    for (auto& h : b->host) {
+        const size_t nv = (size_t)h.G.X * h.G.Y * h.G.Z;
+        h.acc = b->d_acc + off;
+        h.acc_t = b->d_acc + off + nv;
+        off += 2 * nv;
+    }
+    // ray tiles, largest problems (most ray-voxel work) first
+    std::vector<double> work(n);
+    for (int p = 0; p < n; ++p) {
+        const BatchProb& h = b->host[p];
+        work[p] = (double)h.nviews * h.G.Nu * h.G.Nv * (double)(h.G.X + h.G.Y + h.G.Z);
+    }
+    std::vector<int> perm(n);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int c) { return work[a] > work[c]; });
+    std::vector<unsigned long long> ray_prefix(n + 1, 0), tr_prefix(n + 1, 0), vox_prefix(n + 1, 0);
+    for (int q = 0; q < n; ++q) {
+        const BatchProb& h = b->host[perm[q]];
+        ray_prefix[q + 1] = ray_prefix[q] + h.ntiles;
+    }
+    for (int p = 0; p < n; ++p) {
+        const BatchProb& h = b->host[p];
+        tr_prefix[p + 1] = tr_prefix[p] + (unsigned long long)((h.G.X + 31) / 32) * ((h.G.Y + 31) / 32) * h.G.Z;
+        vox_prefix[p + 1] = vox_prefix[p] + (unsigned long long)h.G.X * h.G.Y * h.G.Z;
+    }
+    RB_CHECK(upload(&b->d_ray_prefix, ray_prefix));
+    RB_CHECK(upload(&b->d_tr_prefix, tr_prefix));
+    RB_CHECK(upload(&b->d_vox_prefix, vox_prefix));
+    RB_CUDA(cudaMalloc(&b->d_perm, n * sizeof(int)));
+    RB_CUDA(cudaMemcpy(b->d_perm, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     RB_CUDA(cudaMalloc(&b->d_probs, n * sizeof(BatchProb)));
     RB_CUDA(cudaMalloc(&b->d_counters, 2 * sizeof(unsigned long long)));
     RB_CUDA(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));

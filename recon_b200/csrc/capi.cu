@@ -182,6 +182,8 @@ recon_status_t ensure_mlem_buffers(Plan& P)
         const size_t n = per_view ? P.npix : (size_t)P.nviews * P.npix;
         char* q = nullptr;
         RB_CHECK(P.alloc(&q, n * es, "ratio sinogram"));
+        // zero outside the ray blocks the forward projector writes (EXACT culling)
+        RB_CUDA(cudaMemset(q, 0, n * es));
         P.d_ratio = q;
     }
     return RECON_OK;
@@ -266,7 +268,14 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_zp, geom->det.NumTAxPixels, "ray table z"));
             RB_CHECK(P->alloc(&P->d_w, P->npix, "ray weights"));
             RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
+            const size_t slab = (size_t)P->eg.X * P->eg.Y * bp_slab_depth(*P);
+            RB_CHECK(P->alloc(&P->d_bpacc, slab, "back projection accumulator"));
+            RB_CHECK(P->alloc(&P->d_bpacc_t, slab, "back projection accumulator (transposed)"));
+            RB_CHECK(P->alloc(&P->d_bpmax, 1, "back projection max"));
+            RB_CUDA(cudaMemset(P->d_bpacc, 0, slab * sizeof(unsigned long long)));
+            RB_CUDA(cudaMemset(P->d_bpacc_t, 0, slab * sizeof(unsigned long long)));
             RB_CHECK(build_exact_tables(*P, 0));
+            RB_CHECK(build_exact_culling(*P));
         } else {
             RB_CHECK(P->alloc(&P->d_maxabs, nv1, "maxabs"));
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));

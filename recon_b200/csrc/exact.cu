@@ -19,15 +19,18 @@
 // so the tables are [view][u] for x and y, [v] for z and [v][u] for w.
 //
 // Forward projection: one thread per ray, the voxel walk fully in registers,
-// the step count known before the loop (no exit test on planes).  Back
-// projection: a gather, one thread per (x, y) column and z-chunk; for every
-// view it enumerates the rays crossing its column and accumulates
-// L * value into per-thread shared-memory accumulators in a fixed order
-// (views, then u, then v), so results are bit-reproducible; the MLEM update
-// f <- f * Ht / sens is applied in the epilogue.
+// the step count known before the loop (no exit test on planes); views whose
+// detector rows run along y read an xy-transposed copy of the volume so that
+// a warp's gathers stay coalesced.  Back projection: the same walk per ray,
+// z-slab by z-slab, adding L * value to 64-bit fixed-point accumulators with
+// integer atomics (exact, order-independent sums, so results are
+// bit-reproducible); a finishing pass per slab converts to float and applies
+// the MLEM update f <- f * Ht / sens.
 #include "exact_device.cuh"
 #include "internal.h"
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 
 namespace rb {
@@ -118,17 +121,17 @@ template <bool KAHAN, int MODE, class GT, class OT>
 __global__ void __launch_bounds__(128) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                   const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
                                                   const float* __restrict__ wtab, const float2* __restrict__ cs,
-                                                  unsigned view0, const float* __restrict__ vol,
-                                                  const float* __restrict__ vol_t, const GT* __restrict__ g,
-                                                  OT* __restrict__ out)
+                                                  const uint2* __restrict__ tiles, unsigned view0,
+                                                  const float* __restrict__ vol, const float* __restrict__ vol_t,
+                                                  const GT* __restrict__ g, OT* __restrict__ out)
 {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int v = blockIdx.y * blockDim.y + threadIdx.y;
-    const unsigned view = view0 + blockIdx.z;
+    const RayPos R = ray_pos(tiles, view0);
+    const int u = R.u, v = R.v;
+    const unsigned view = R.view;
     if (u >= G.Nu || v >= G.Nv) return;
     const VolView V = vol_view_for(__ldg(cs + view), vol, vol_t, G.X, G.Y);
     const size_t pix = (size_t)u + (size_t)v * G.Nu;
-    const size_t n = (size_t)blockIdx.z * G.Nu * G.Nv + pix;
+    const size_t n = (size_t)(view - view0) * G.Nu * G.Nv + pix;
     const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
     const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
     const ZParam Z = zp[v];
@@ -145,54 +148,74 @@ __global__ void __launch_bounds__(128) fp_kernel(ExactGeom G, const float4* __re
     }
 }
 
-// ---- back projection (gather) ------------------------------------------------------------
+// ---- back projection (ray-driven, into a z-slab) ---------------------------------------------
 
-// MODE 0: vol = Ht (back projection of the sinogram)
-// MODE 1: vol = sensitivity (back projection of ones)
-// MODE 2: f = (sens != 0) ? f*Ht/sens : 0 (MLEM update, in place)
-// WEIGHTED: sinogram values are plain (multiply by w); otherwise they already
-// carry w (the MLEM ratio written by the forward kernel).
-template <int ZC, int MODE, bool WEIGHTED, class ST>
-__global__ void __launch_bounds__(128) bp_kernel(ExactGeom G, const float4* __restrict__ txy,
-                                                  const int2* __restrict__ kxy, const float2* __restrict__ cs,
-                                                  const ZParam* __restrict__ zp, const float* __restrict__ wtab,
-                                                  unsigned view0, unsigned nview, const ST* __restrict__ sino,
-                                                  float* __restrict__ vol, const float* __restrict__ sens)
+// MODE 0: sinogram values (times w when WEIGHTED; the MLEM ratio already
+// carries w); MODE 1: the value is w (the sensitivity).  One thread per ray
+// (ray_pos), rays with a zero value skipped; sino holds views from view0 on.
+template <int MODE, bool WEIGHTED, class ST>
+__global__ void __launch_bounds__(128) bp_ray_kernel(ExactGeom G, const float4* __restrict__ txy,
+                                                      const int2* __restrict__ kxy, const float2* __restrict__ cs,
+                                                      const ZParam* __restrict__ zp, const float* __restrict__ wtab,
+                                                      const uint2* __restrict__ tiles, unsigned view0,
+                                                      const ST* __restrict__ sino,
+                                                      const unsigned* __restrict__ maxabs, float max_len,
+                                                      int count_bits, int k0, int k1, unsigned long long* acc,
+                                                      unsigned long long* acc_t)
 {
-    extern __shared__ float smem[];
-    float* acc = smem;                                         // [ZC][128]
-    float4* szb = reinterpret_cast<float4*>(smem + ZC * 128);  // [Nv] mirrored z planes
-    const int tid = threadIdx.x + threadIdx.y * 32;
-    for (int q = tid; q < G.Nv; q += 128) {
-        const ZParam z = zp[q];
-        const bool pos = z.S > 0.0f;
-        szb[q] = make_float4(fabsf(z.S), pos ? z.O : -z.O, (float)z.kc, pos ? 1.0f : -1.0f);
-    }
-#pragma unroll
-    for (int q = 0; q < ZC; ++q) acc[q * 128 + tid] = 0.0f;
-    __syncthreads();
+    const RayPos R = ray_pos(tiles, view0);
+    const int u = R.u, v = R.v;
+    const unsigned view = R.view;
+    if (u >= G.Nu || v >= G.Nv) return;
+    const int F = fix_exponent(*maxabs, max_len, count_bits);
+    if (F == INT_MIN) return;
+    const size_t pix = (size_t)u + (size_t)v * G.Nu;
+    float val;
+    if (MODE == 1) val = __ldg(wtab + pix);
+    else val = load_val<ST>(sino + (size_t)(view - view0) * G.Nu * G.Nv + pix);
+    if (WEIGHTED && MODE != 1) val *= __ldg(wtab + pix);
+    if (val == 0.0f) return;
+    const float2 C = __ldg(cs + view);
+    bp_ray_slab(G, __ldg(txy + (size_t)view * G.Nu + u), __ldg(kxy + (size_t)view * G.Nu + u), zp[v], k0, k1,
+                val * ldexpf(1.0f, F), fabsf(C.y) > fabsf(C.x), acc, acc_t);
+}
 
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 4 + threadIdx.y;
-    const int k0 = blockIdx.z * ZC;
-    const int k1 = min(k0 + ZC, G.Z);
-    const bool active = (i < G.X) && (j < G.Y);
-    if (active) {
-        bp_gather_column<ZC, MODE, WEIGHTED, ST>(G, txy, kxy, cs, wtab, view0, nview, sino, szb, acc, tid, i, j,
-                                                 k0, k1);
-        // epilogue
-        for (int k = k0; k < k1; ++k) {
-            const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)k * G.X * G.Y;
-            const float ht = acc[(k - k0) * 128 + tid];
-            if (MODE == 2) {
-                const float s = sens[vox];
-                const float f = vol[vox];
-                vol[vox] = (s != 0.0f) ? __fdiv_rn(__fmul_rn(f, ht), s) : 0.0f;
-            } else {
-                vol[vox] = ht;
-            }
+// Slab [k0, k1) of the result from the accumulators:
+// MODE 0: vol = Ht; MODE 2: f = (sens != 0) ? f * Ht / sens : 0 (MLEM update).
+template <int MODE>
+__global__ void bp_finish_kernel(ExactGeom G, const unsigned* __restrict__ maxabs, float max_len, int count_bits,
+                                 int k0, int k1, unsigned long long* acc, unsigned long long* acc_t,
+                                 float* __restrict__ vol, const float* __restrict__ sens)
+{
+    const int F = fix_exponent(*maxabs, max_len, count_bits);
+    const size_t plane = (size_t)G.X * G.Y, n = plane * (size_t)(k1 - k0);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % G.X), y = (int)((i / G.X) % G.Y), zs = (int)(i / plane);
+        const float ht = bp_slab_value(G, x, y, zs, F, acc, acc_t);
+        const size_t vox = i + (size_t)k0 * plane;
+        if (MODE == 2) {
+            const float sv = sens[vox];
+            vol[vox] = (sv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[vox], ht), sv) : 0.0f;
+        } else {
+            vol[vox] = ht;
         }
     }
+}
+
+// max |value| (times w when w != nullptr) over n values, as float bits, into
+// *out (atomicMax of non-negative floats ordered as unsigned integers)
+template <class ST>
+__global__ void maxabs_kernel(const ST* __restrict__ a, size_t n, const float* __restrict__ w, size_t npix,
+                              unsigned* __restrict__ out)
+{
+    unsigned m = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float v = fabsf(load_val<ST>(a + i));
+        if (w) v *= __ldg(w + i % npix);
+        m = max(m, __float_as_uint(v));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
 }  // namespace exact
@@ -279,22 +302,123 @@ recon_status_t exact_transpose(const float* vol, float* vol_t, int X, int Y, int
     return RECON_OK;
 }
 
+// ---- ray culling ---------------------------------------------------------------------------
+
+namespace exact {
+// Bounding rectangle {u_min, u_max, v_min, v_max} per view of the rays that
+// cross the box x in [0, X), y in [0, Y), z in [k0, k1): the clip test of the
+// walks themselves, so no ray with a non-empty walk falls outside.
+__global__ void __launch_bounds__(128) hit_rect_kernel(ExactGeom G, const float4* __restrict__ txy,
+                                                        const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
+                                                        int k0, int k1, int4* __restrict__ rect)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y * blockDim.y + threadIdx.y;
+    const unsigned view = blockIdx.z;
+    if (u >= G.Nu || v >= G.Nv) return;
+    const float4 T = txy[(size_t)view * G.Nu + u];
+    const int2 K = kxy[(size_t)view * G.Nu + u];
+    const ZParam Z = zp[v];
+    const float x0 = plane_t(0, T.x, T.y, K.x), x1 = plane_t(G.X, T.x, T.y, K.x);
+    const float y0 = plane_t(0, T.z, T.w, K.y), y1 = plane_t(G.Y, T.z, T.w, K.y);
+    const float z0 = plane_t(k0, Z.S, Z.O, Z.kc), z1 = plane_t(k1, Z.S, Z.O, Z.kc);
+    const float t_in = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fminf(z0, z1));
+    const float t_out = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fmaxf(z0, z1));
+    if (!(t_in < t_out)) return;
+    atomicMin(&rect[view].x, u);
+    atomicMax(&rect[view].y, u);
+    atomicMin(&rect[view].z, v);
+    atomicMax(&rect[view].w, v);
+}
+}  // namespace exact
+
+// Tile list of the 32x4 ray blocks inside each plan view's rectangle of rays
+// crossing the box z in [k0, k1).  Synchronous (plan creation).
+static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T)
+{
+    const unsigned nv = P.nviews;
+    T.prefix.assign(nv + 1, 0);
+    if (nv == 0) return RECON_OK;
+    std::vector<int4> rect(nv, make_int4(INT_MAX, -1, INT_MAX, -1));
+    int4* d_rect = nullptr;
+    RB_CUDA(cudaMalloc(&d_rect, nv * sizeof(int4)));
+    cudaError_t e = cudaMemcpy(d_rect, rect.data(), nv * sizeof(int4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        exact::hit_rect_kernel<<<fp_grid(P, nv), fp_block()>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, k0, k1, d_rect);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(rect.data(), d_rect, nv * sizeof(int4), cudaMemcpyDeviceToHost);
+    cudaFree(d_rect);
+    if (e != cudaSuccess) return cuda_fail(e, "ray culling");
+    std::vector<uint2> tiles;
+    for (unsigned n = 0; n < nv; ++n) {
+        T.prefix[n] = (unsigned)tiles.size();
+        const int4 r = rect[n];
+        if (r.y < r.x) continue;  // no ray of this view crosses the box
+        for (int tv = r.z / 4; tv <= r.w / 4; ++tv)
+            for (int tu = r.x / 32; tu <= r.y / 32; ++tu) tiles.push_back(make_uint2(n, (unsigned)tu | ((unsigned)tv << 16)));
+    }
+    T.prefix[nv] = (unsigned)tiles.size();
+    if (tiles.empty()) return RECON_OK;
+    RB_CHECK(P.alloc(&T.d, tiles.size(), "ray tiles"));
+    RB_CUDA(cudaMemcpy(T.d, tiles.data(), tiles.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    return RECON_OK;
+}
+
+recon_status_t build_exact_culling(Plan& P)
+{
+    RB_CHECK(build_ray_tiles(P, 0, P.eg.Z, P.fp_tiles));
+    P.bp_tiles.clear();
+    const int depth = bp_slab_depth(P);
+    for (int k0 = 0; k0 < P.eg.Z; k0 += depth) {
+        P.bp_tiles.emplace_back();
+        RB_CHECK(build_ray_tiles(P, k0, std::min(k0 + depth, P.eg.Z), P.bp_tiles.back()));
+    }
+    return RECON_OK;
+}
+
+// Launch shape for views [first, first+count): the tiles of `T` when those
+// are plan views (culled), else the full grid.  *tiles is null for the full
+// grid; *n_launch = 0 when no ray can contribute.
+static void ray_launch(const Plan& P, const RayTiles& T, unsigned first, unsigned count, dim3* grid,
+                       const uint2** tiles, unsigned* n_launch)
+{
+    if (first + count <= P.nviews && T.prefix.size() == P.nviews + 1) {
+        const unsigned t0 = T.prefix[first], nt = T.prefix[first + count] - t0;
+        *grid = dim3(std::max(nt, 1u), 1, 1);
+        *tiles = T.d + t0;
+        *n_launch = nt;
+    } else {
+        *grid = fp_grid(P, count);
+        *tiles = nullptr;
+        *n_launch = count;
+    }
+}
+
 // Forward projection of views [first, first+count) (table slots), reading the
 // volume in the layout that suits each view (the transposed copy is made
-// here, once per call).
+// here, once per call).  Only ray blocks that can cross the volume are
+// launched; the other pixels of `out` are zeroed first, except for the MLEM
+// ratio (MODE 1), whose buffer is zero outside the blocks from allocation on.
 template <int MODE, class GT, class OT>
 static recon_status_t launch_fp(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g, OT* out,
                                 cudaStream_t s)
 {
     if (count == 0) return RECON_OK;
+    dim3 grid;
+    const uint2* tiles;
+    unsigned n_launch;
+    ray_launch(P, P.fp_tiles, first, count, &grid, &tiles, &n_launch);
+    if (tiles && MODE != 1) RB_CUDA(cudaMemsetAsync(out, 0, (size_t)count * P.npix * sizeof(OT), s));
+    if (n_launch == 0) return RECON_OK;
     RB_CHECK(exact_transpose(vol, P.d_vol_t, P.eg.X, P.eg.Y, P.eg.Z, s));
-    const dim3 grid = fp_grid(P, count), blk = fp_block();
+    const dim3 blk = fp_block();
     if (P.opt.sum == RECON_SUM_KAHAN)
         exact::fp_kernel<true, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
-                                                                  first, vol, P.d_vol_t, g, out);
+                                                                  tiles, first, vol, P.d_vol_t, g, out);
     else
         exact::fp_kernel<false, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
-                                                                   first, vol, P.d_vol_t, g, out);
+                                                                   tiles, first, vol, P.d_vol_t, g, out);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
@@ -324,11 +448,12 @@ recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ra
 namespace exact {
 __global__ void __launch_bounds__(128) count_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                      const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
+                                                     const uint2* __restrict__ tiles,
                                                      unsigned long long* __restrict__ total)
 {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int v = blockIdx.y * blockDim.y + threadIdx.y;
-    const unsigned view = blockIdx.z;
+    const RayPos R = ray_pos(tiles, 0u);
+    const int u = R.u, v = R.v;
+    const unsigned view = R.view;
     unsigned cnt = 0;
     if (u < G.Nu && v < G.Nv) {
         const float4 T = txy[(size_t)view * G.Nu + u];
@@ -379,8 +504,14 @@ recon_status_t exact_count(Plan& P, unsigned long long* out)
     RB_CUDA(cudaMalloc(&d, sizeof(unsigned long long)));
     cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
     if (e == cudaSuccess && P.nviews) {
-        exact::count_kernel<<<fp_grid(P, P.nviews), fp_block()>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, d);
-        e = cudaGetLastError();
+        dim3 grid;
+        const uint2* tiles;
+        unsigned n_launch;
+        ray_launch(P, P.fp_tiles, 0, P.nviews, &grid, &tiles, &n_launch);
+        if (n_launch) {
+            exact::count_kernel<<<grid, fp_block()>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, tiles, d);
+            e = cudaGetLastError();
+        }
     }
     if (e == cudaSuccess) e = cudaMemcpy(out, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
     cudaFree(d);
@@ -393,17 +524,78 @@ recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, f
     return launch_fp<2, float, float>(P, vol, 0u, P.nviews, g, ratio, s);
 }
 
-template <int ZC, int MODE, bool WEIGHTED, class ST>
+// Bound on the number of contributions one voxel receives from `nview`
+// views, as bits: a voxel's projection is at most diag * Ry / depth_min
+// detector pitches wide in u and in v, so at most floor(w) + 2 pixel centres
+// per axis see it.
+int bp_count_bits(const Plan& P, unsigned nview)
+{
+    const ExactGeom& E = P.eg;
+    const double vx = E.vox[0], vy = E.vox[1], vz = E.vox[2];
+    const double diag = std::sqrt(vx * vx + vy * vy + vz * vz);
+    const double hx = 0.5 * E.X * vx, hy = 0.5 * E.Y * vy, hz = 0.5 * E.Z * vz;
+    const double depth_min = std::max((double)E.Rf - std::sqrt(hx * hx + hy * hy + hz * hz), 1e-3);
+    const double mag = std::fabs((double)E.Ry) / depth_min;
+    const double fu = diag * mag / std::fabs((double)E.du), fv = diag * mag / std::fabs((double)E.dv);
+    const double total = (double)std::max(nview, 1u) * (std::floor(fu) + 2.0) * (std::floor(fv) + 2.0);
+    return (int)std::ceil(std::log2(total)) + 1;
+}
+
+// Longest segment in t: a segment's length in t is at most its length in
+// mm (the source-to-pixel distance is at least R), at most a voxel diagonal.
+float bp_max_len(const Plan& P)
+{
+    const ExactGeom& E = P.eg;
+    return (float)(std::sqrt((double)E.vox[0] * E.vox[0] + (double)E.vox[1] * E.vox[1] +
+                             (double)E.vox[2] * E.vox[2]) * 1.0001);
+}
+
+// z-slices per slab: both accumulators of a slab (16 bytes per voxel) in
+// about 64 MiB, which stays resident in the 126 MB L2.
+int bp_slab_depth(const Plan& P)
+{
+    const size_t per_slice = (size_t)P.eg.X * P.eg.Y * 2 * sizeof(unsigned long long);
+    return (int)std::max<size_t>(1, std::min<size_t>((size_t)P.eg.Z, (size_t(64) << 20) / per_slice));
+}
+
+template <int MODE, bool WEIGHTED, class ST>
 static recon_status_t launch_bp(Plan& P, const ST* sino, unsigned first, unsigned count, float* vol,
                                 const float* sens, cudaStream_t s)
 {
-    const size_t smem = (size_t)ZC * 128 * sizeof(float) + (size_t)P.eg.Nv * sizeof(ZParam);
-    auto kern = exact::bp_kernel<ZC, MODE, WEIGHTED, ST>;
-    RB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((P.eg.X + 31) / 32, (P.eg.Y + 3) / 4, (P.eg.Z + ZC - 1) / ZC);
-    kern<<<grid, dim3(32, 4, 1), smem, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_cs, P.d_zp, P.d_w, first, count, sino, vol,
-                                             sens);
+    // max |value| of this call's input, for the fixed-point scale
+    RB_CUDA(cudaMemsetAsync(P.d_bpmax, 0, sizeof(unsigned), s));
+    const size_t n = (MODE == 1) ? P.npix : (size_t)count * P.npix;
+    const unsigned mblocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)P.sm_count * 8);
+    if (MODE == 1)
+        exact::maxabs_kernel<float><<<mblocks, 256, 0, s>>>(P.d_w, n, nullptr, P.npix, P.d_bpmax);
+    else
+        exact::maxabs_kernel<ST><<<mblocks, 256, 0, s>>>(sino, n, WEIGHTED ? P.d_w : nullptr, P.npix, P.d_bpmax);
     RB_CUDA(cudaGetLastError());
+    const float max_len = bp_max_len(P);
+    const int cbits = bp_count_bits(P, count);
+    const int depth = bp_slab_depth(P);
+    const dim3 blk = fp_block();
+    const unsigned fblocks = (unsigned)P.sm_count * 8;
+    constexpr int RMODE = (MODE == 1) ? 1 : 0;
+    const RayTiles none;
+    for (int k0 = 0, slab = 0; k0 < P.eg.Z; k0 += depth, ++slab) {
+        const int k1 = std::min(k0 + depth, P.eg.Z);
+        dim3 grid;
+        const uint2* tiles;
+        unsigned n_launch;
+        ray_launch(P, slab < (int)P.bp_tiles.size() ? P.bp_tiles[slab] : none, first, count, &grid, &tiles,
+                   &n_launch);
+        if (n_launch) {
+            exact::bp_ray_kernel<RMODE, WEIGHTED, ST><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_cs, P.d_zp,
+                                                                           P.d_w, tiles, first, sino, P.d_bpmax,
+                                                                           max_len, cbits, k0, k1, P.d_bpacc,
+                                                                           P.d_bpacc_t);
+            RB_CUDA(cudaGetLastError());
+        }
+        exact::bp_finish_kernel<MODE == 2 ? 2 : 0><<<fblocks, 256, 0, s>>>(P.eg, P.d_bpmax, max_len, cbits, k0, k1,
+                                                                           P.d_bpacc, P.d_bpacc_t, vol, sens);
+        RB_CUDA(cudaGetLastError());
+    }
     return RECON_OK;
 }
 
@@ -415,15 +607,15 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
         first = P.nviews;
         count = 1;
     }
-    constexpr int ZC = 32;
+    if (count == 0) return launch_fill(f_update ? f_update : vol, 0.0f, P.nvox, s);
     using bf = __nv_bfloat16;
-    if (sens_mode) return launch_bp<ZC, 1, false, float>(P, nullptr, first, count, vol, nullptr, s);
+    if (sens_mode) return launch_bp<1, false, float>(P, nullptr, first, count, vol, nullptr, s);
     if (f_update) {
-        if (bf16) return launch_bp<ZC, 2, false, bf>(P, (const bf*)sino, first, count, f_update, sens, s);
-        return launch_bp<ZC, 2, false, float>(P, (const float*)sino, first, count, f_update, sens, s);
+        if (bf16) return launch_bp<2, false, bf>(P, (const bf*)sino, first, count, f_update, sens, s);
+        return launch_bp<2, false, float>(P, (const float*)sino, first, count, f_update, sens, s);
     }
-    if (sino_is_rw) return launch_bp<ZC, 0, false, float>(P, (const float*)sino, first, count, vol, nullptr, s);
-    return launch_bp<ZC, 0, true, float>(P, (const float*)sino, first, count, vol, nullptr, s);
+    if (sino_is_rw) return launch_bp<0, false, float>(P, (const float*)sino, first, count, vol, nullptr, s);
+    return launch_bp<0, true, float>(P, (const float*)sino, first, count, vol, nullptr, s);
 }
 
 }  // namespace rb

@@ -5,6 +5,8 @@
 
 #include <cuda_bf16.h>
 
+#include <climits>
+
 #include "internal.h"
 
 namespace rb {
@@ -50,6 +52,26 @@ template <>
 __device__ __forceinline__ void store_val<float>(float* p, float v) { *p = v; }
 template <>
 __device__ __forceinline__ void store_val<__nv_bfloat16>(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+
+// ---- ray blocks ---------------------------------------------------------------------------
+
+// Rays are launched in blocks of 32 (u) x 4 (v).  A CTA's block comes from a
+// tile list ({view, tu | tv << 16}, the blocks whose rays can cross the
+// volume; blockIdx.x indexes it) or, when tiles is null, from the full grid
+// (blockIdx.x, blockIdx.y, view view0 + blockIdx.z).
+struct RayPos {
+    int u, v;
+    unsigned view;
+};
+
+__device__ __forceinline__ RayPos ray_pos(const uint2* __restrict__ tiles, unsigned view0)
+{
+    if (tiles) {
+        const uint2 t = tiles[blockIdx.x];
+        return RayPos{(int)(t.y & 0xffffu) * 32 + (int)threadIdx.x, (int)(t.y >> 16) * 4 + (int)threadIdx.y, t.x};
+    }
+    return RayPos{(int)(blockIdx.x * 32 + threadIdx.x), (int)(blockIdx.y * 4 + threadIdx.y), view0 + blockIdx.z};
+}
 
 // ---- forward projection --------------------------------------------------------------------
 
@@ -132,94 +154,95 @@ __device__ __forceinline__ float fp_ray_sum(const ExactGeom& G, const float4 T, 
     return acc;
 }
 
-// Gather of views [view0, view0+nview) into the ZC accumulators of column
-// (i, j), voxels k0..k1-1 (acc[(k-k0)*128 + tid] in shared memory).  sino holds
-// the views' values, view vi at sino + vi*Nv*Nu; szb the mirrored z planes.
-template <int ZC, int MODE, bool WEIGHTED, class ST>
-__device__ __forceinline__ void bp_gather_column(const ExactGeom& G, const float4* __restrict__ txy,
-                                                 const int2* __restrict__ kxy, const float2* __restrict__ cs,
-                                                 const float* __restrict__ wtab, unsigned view0, unsigned nview,
-                                                 const ST* __restrict__ sino, const float4* szb, float* acc,
-                                                 int tid, int i, int j, int k0, int k1)
+// ---- back projection (ray-driven, exact fixed-point sums) -----------------------------------
+//
+// Each ray walks the voxels it crosses exactly as the forward projector does,
+// restricted to a z-slab [k0, k1) of the volume, and adds L * value to each
+// voxel's 64-bit fixed-point accumulator with an integer atomic.  Integer sums
+// do not depend on the order of the additions, so the result is
+// deterministic, and every (ray, voxel) length is the forward projector's, so
+// the pair is an exact transpose.  The scale 2^F is chosen per call so that
+// no voxel sum can overflow: |L * value| < 2^e (max |value| times the longest
+// segment) and at most 2^count_bits contributions per voxel give
+// |sum| < 2^(e + F + count_bits) = 2^62.  A slab's accumulators are sized to
+// stay resident in L2.  Views whose detector rows run mostly along y add into
+// a second, xy-transposed accumulator, so that the 32 rays of a warp (adjacent
+// detector columns) update adjacent addresses in either case.
+
+// F for the fixed-point scale, or INT_MIN when the input is all zero or not
+// finite (nothing is accumulated then).
+__device__ __forceinline__ int fix_exponent(unsigned maxabs_bits, float max_len, int count_bits)
 {
-    const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
-    const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
-    const float Za = G.P0[2] + k0 * G.vox[2], Zb = G.P0[2] + k1 * G.vox[2];
-    const float RyR = G.Ry / G.R;
-    const float inv_du = 1.0f / G.du, inv_dv = 1.0f / G.dv;
-    for (unsigned vi = 0; vi < nview; ++vi) {
-        const unsigned view = view0 + vi;
-        const float2 CS = __ldg(cs + view);
-        // detector u range of the column: project its four corners
-        float umin = 3.0e38f, umax = -3.0e38f;
-#pragma unroll
-        for (int c4 = 0; c4 < 4; ++c4) {
-            const float X = (c4 & 1) ? Xb : Xa, Y = (c4 & 2) ? Yb : Ya;
-            const float xv = X * CS.x - Y * CS.y, yv = X * CS.y + Y * CS.x;
-            const float ud = __fdividef(G.R * xv, yv + G.Rf) * RyR - G.Dx;  // candidates only
-            const float uf = (ud - G.ud0) * inv_du;
-            umin = fminf(umin, uf);
-            umax = fmaxf(umax, uf);
-        }
-        const int u_lo = max(0, (int)ceilf(umin - 2e-3f));
-        const int u_hi = min(G.Nu - 1, (int)floorf(umax + 2e-3f));
-        for (int u = u_lo; u <= u_hi; ++u) {
-            const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
-            const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
-            const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
-            const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
-            const float A = fmaxf(fminf(xa, xb), fminf(ya, yb));
-            const float B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
-            if (!(A < B)) continue;
-            // rows v whose ray can cross the z-chunk inside [A, B]
-            // (candidates only, with a margin): z = vd * (t + Rf) / R
-            const float ra = __fdividef(G.R, A + G.Rf), rb = __fdividef(G.R, B + G.Rf);
-            const float c1 = Za * ra, c2 = Za * rb, c3 = Zb * ra, c4 = Zb * rb;
-            const float vdmin = fminf(fminf(c1, c2), fminf(c3, c4));
-            const float vdmax = fmaxf(fmaxf(c1, c2), fmaxf(c3, c4));
-            const float vfa = (vdmin * RyR - G.Dz - G.vd0) * inv_dv;
-            const float vfb = (vdmax * RyR - G.Dz - G.vd0) * inv_dv;
-            const int v_lo = max(0, (int)ceilf(fminf(vfa, vfb) - 2e-3f));
-            const int v_hi = min(G.Nv - 1, (int)floorf(fmaxf(vfa, vfb) + 2e-3f));
-            const ST* srow = sino + ((size_t)vi * G.Nv) * G.Nu + u;
-            // Sweep the needles (the rays' pieces inside this column) in
-            // increasing z together with the chunk's voxels.  The lowest
-            // voxel a needle touches never decreases from one needle to
-            // the next, so k carries over.  Each ray's z planes are
-            // mirrored (t -> -t for rays going down, exact in IEEE) so
-            // that T(k) increases with k for every ray:
-            //   L(v, k) = min(B', T(k+1)) - max(A', T(k)).
-            int k = k0;
-            for (int v = v_lo; v <= v_hi; ++v) {
-                const float4 Z = szb[v];  // {|S|, sign(S)*O, kc, sign(S)}
-                float val;
-                if (MODE == 1) val = __ldg(wtab + (size_t)v * G.Nu + u);
-                else val = load_val<ST>(srow + (size_t)v * G.Nu);
-                if (WEIGHTED && MODE != 1) val *= __ldg(wtab + (size_t)v * G.Nu + u);
-                const float Ap = Z.w > 0.0f ? A : -B;
-                const float Bp = Z.w > 0.0f ? B : -A;
-                float kf = (float)k;
-                float T1 = fmaf(kf + 1.0f - Z.z, Z.x, Z.y);
-                while (T1 <= Ap && k < k1) {  // voxel k lies wholly before the needle
-                    ++k;
-                    kf += 1.0f;
-                    T1 = fmaf(kf + 1.0f - Z.z, Z.x, Z.y);
-                }
-                if (k >= k1) break;  // this and every later needle lie above the chunk
-                float T0 = fmaf(kf - Z.z, Z.x, Z.y);
-                float* a = acc + (k - k0) * 128 + tid;
-#pragma unroll 1
-                for (int kk = k;;) {
-                    const float L = fminf(Bp, T1) - fmaxf(Ap, T0);
-                    if (L > 0.0f) *a = fmaf(L, val, *a);
-                    if (T1 >= Bp || ++kk >= k1) break;
-                    a += 128;
-                    T0 = T1;
-                    T1 = fmaf((float)kk + 1.0f - Z.z, Z.x, Z.y);
-                }
-            }
-        }
+    const float m = __uint_as_float(maxabs_bits);
+    if (!(m > 0.0f) || !isfinite(m)) return INT_MIN;
+    int e;
+    frexp((double)m * (double)max_len, &e);
+    return min(62 - count_bits - e, 120);
+}
+
+// One ray's contributions to the slab [k0, k1): cval = value * 2^F.  acc is
+// the slab in image layout [z-k0][y][x]; acc_t the transposed one
+// [z-k0][x][y], used when `transposed`.
+__device__ __forceinline__ void bp_ray_slab(const ExactGeom& G, const float4 T, const int2 K, const ZParam Z,
+                                            int k0, int k1, float cval, bool transposed, unsigned long long* acc,
+                                            unsigned long long* acc_t)
+{
+    const float x0 = plane_t(0, T.x, T.y, K.x), x1 = plane_t(G.X, T.x, T.y, K.x);
+    const float y0 = plane_t(0, T.z, T.w, K.y), y1 = plane_t(G.Y, T.z, T.w, K.y);
+    const float z0 = plane_t(k0, Z.S, Z.O, Z.kc), z1 = plane_t(k1, Z.S, Z.O, Z.kc);
+    const float t_in = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fminf(z0, z1));
+    const float t_out = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fmaxf(z0, z1));
+    if (!(t_in < t_out)) return;
+    const double ivx = 1.0 / (double)T.x, ivy = 1.0 / (double)T.z, ivz = 1.0 / (double)Z.S;
+    const int ix = locate<true>(t_in, T.x, T.y, K.x, G.X, ivx), ex = locate<false>(t_out, T.x, T.y, K.x, G.X, ivx);
+    const int iy = locate<true>(t_in, T.z, T.w, K.y, G.Y, ivy), ey = locate<false>(t_out, T.z, T.w, K.y, G.Y, ivy);
+    const int iz = min(max(locate<true>(t_in, Z.S, Z.O, Z.kc, G.Z, ivz), k0), k1 - 1);
+    const int ez = min(max(locate<false>(t_out, Z.S, Z.O, Z.kc, G.Z, ivz), k0), k1 - 1);
+    const int nsteps = abs(ex - ix) + abs(ey - iy) + abs(ez - iz) + 1;
+    const int dx = T.x > 0.0f ? 1 : -1, dy = T.z > 0.0f ? 1 : -1, dz = Z.S > 0.0f ? 1 : -1;
+    float kx = (float)((dx > 0 ? ix + 1 : ix) - K.x);
+    float ky = (float)((dy > 0 ? iy + 1 : iy) - K.y);
+    float kz = (float)((dz > 0 ? iz + 1 : iz) - Z.kc);
+    float tx = fmaf(kx, T.x, T.y), ty = fmaf(ky, T.z, T.w), tz = fmaf(kz, Z.S, Z.O);
+    const float fdx = (float)dx, fdy = (float)dy, fdz = (float)dz;
+    const int ux = transposed ? G.Y : 1, uy = transposed ? 1 : G.X;
+    unsigned long long* __restrict__ A = transposed ? acc_t : acc;
+    const int sx = dx * ux, sy = dy * uy, sz = dz * G.X * G.Y;
+    const unsigned lmax = (unsigned)(G.X * G.Y * (k1 - k0) - 1);
+    int l = ix * ux + iy * uy + (iz - k0) * G.X * G.Y;
+    float cur = t_in;
+#pragma unroll 2
+    for (int s = 0; s < nsteps; ++s) {
+        const float m = fminf(tx, fminf(ty, tz));
+        const long long q = __float2ll_rn((m - cur) * cval);
+        if (q != 0) atomicAdd(A + min((unsigned)l, lmax), (unsigned long long)q);
+        cur = m;
+        // advance the axis whose plane was crossed (x before y before z on
+        // ties), as the forward walk does
+        const bool bx = (tx == m);
+        const bool by = !bx && (ty == m);
+        const bool bz = !bx && !by;
+        kx = bx ? kx + fdx : kx;
+        ky = by ? ky + fdy : ky;
+        kz = bz ? kz + fdz : kz;
+        tx = bx ? fmaf(kx, T.x, T.y) : tx;
+        ty = by ? fmaf(ky, T.z, T.w) : ty;
+        tz = bz ? fmaf(kz, Z.S, Z.O) : tz;
+        l += bx ? sx : (by ? sy : sz);
     }
+}
+
+// Fixed point -> float for voxel (x, y, z) of the slab starting at k0:
+// the sum of both accumulators, which are cleared for the next use.
+__device__ __forceinline__ float bp_slab_value(const ExactGeom& G, int x, int y, int zs, int F,
+                                               unsigned long long* acc, unsigned long long* acc_t)
+{
+    const size_t a = (size_t)x + (size_t)y * G.X + (size_t)zs * G.X * G.Y;
+    const size_t b = (size_t)y + (size_t)x * G.Y + (size_t)zs * G.X * G.Y;
+    const long long q = (long long)(acc[a] + acc_t[b]);
+    acc[a] = 0ull;
+    acc_t[b] = 0ull;
+    return (F != INT_MIN) ? (float)ldexp((double)q, -F) : 0.0f;
 }
 
 }  // namespace exact

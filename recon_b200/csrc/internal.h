@@ -75,6 +75,14 @@ struct DeviceBuf {
     size_t bytes = 0;
 };
 
+// Blocks of 32 x 4 rays that can cross a box of the volume: tiles
+// {view, tu | tv << 16} in view order, prefix[n] = index of view n's first
+// tile (prefix has nviews + 1 entries).
+struct RayTiles {
+    uint2* d = nullptr;
+    std::vector<unsigned> prefix;
+};
+
 struct Plan {
     recon_geometry_t geom{};
     recon_options_t opt{};
@@ -95,6 +103,15 @@ struct Plan {
     ZParam* d_zp = nullptr;    // [v]
     float* d_w = nullptr;      // [v][u] |p2-p1| / R
     float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y]
+    // back projection: fixed-point accumulators of one z-slab, image layout
+    // and xy-transposed, and the max |value| of the call's input (float bits)
+    unsigned long long* d_bpacc = nullptr;
+    unsigned long long* d_bpacc_t = nullptr;
+    unsigned* d_bpmax = nullptr;
+    // ray blocks crossing the volume (forward projection) and each
+    // back-projection z-slab; rays outside them contribute nothing
+    RayTiles fp_tiles;
+    std::vector<RayTiles> bp_tiles;
     // scratch view slot for arbitrary-angle single-view calls (index nviews)
     float* d_angles = nullptr;    // [view] (float)n*DeltaAng, + 1 scratch slot
     // COMPAT tables
@@ -170,6 +187,10 @@ recon_status_t ensure_mlem_buffers(Plan& P);
 recon_status_t compute_sensitivity(Plan& P, float* sens, cudaStream_t s);
 recon_status_t describe_compat_geometry(const recon_geometry_t& g, Plan& P);
 recon_status_t exact_transpose(const float* vol, float* vol_t, int X, int Y, int Z, cudaStream_t s);
+int bp_count_bits(const Plan& P, unsigned nview);
+float bp_max_len(const Plan& P);
+int bp_slab_depth(const Plan& P);
+recon_status_t build_exact_culling(Plan& P);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);
 recon_status_t launch_update(float* f, const float* ht, const float* sens, size_t n, bool fast_div,
