@@ -45,6 +45,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-steps", type=int, default=24)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain leg")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched-vs-plain leg and print it as the JSON line")
     ap.add_argument("--batched-problems", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=20)
     return ap.parse_args()
@@ -297,6 +299,14 @@ def main():
     from recon_b200.sharding import ordered_sum_, view_range
 
     world, rank, local = dist_env()
+    if args.batched_only:
+        torch.cuda.set_device(local)
+        opts = Options(sum=SUM_KAHAN if args.sum == "kahan" else SUM_PLAIN, device=local)
+        leg = batched_leg(torch.device("cuda", local), args.batched_problems, args.batched_iters, opts)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": leg["batched_iter_s"], "unit": "MLEM iter/s (problem-iterations)",
+                              "n_gpus": 1, "higher_is_better": True, "batched": leg}))
+        return
     if world > 1:
         import datetime
 

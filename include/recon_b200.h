@@ -88,9 +88,10 @@ typedef struct {
 /* Arithmetic of the Siddon projector pair.
  *   RECON_ARITH_EXACT  -- true Siddon: every ray-voxel intersection length,
  *     plane crossings set up in FP64 and traversed in FP32, forward and back
- *     projectors exact transposes of each other, back projection a
- *     deterministic gather.  Detector tilt angles (xangle/yangle/zangle) must
- *     be zero.
+ *     projectors exact transposes of each other (the same walk per ray), back
+ *     projection summed exactly in 64-bit fixed point, so it is
+ *     deterministic.  Detector tilt angles (xangle/yangle/zangle) must be
+ *     zero.
  *   RECON_ARITH_COMPAT -- the reference's FP32 traversal reproduced operation
  *     for operation (siddon_kernelsMLEM.cuh), including its quirks; per-ray
  *     voxel/length sequences are bit-identical to the reference's kernels on
@@ -224,21 +225,23 @@ recon_status_t recon_mlem_backward_update(recon_plan_t plan, float* d_f, void* s
 
 /* ---- batches of independent reconstructions ------------------------------ */
 
-/* Many MLEM problems (each its own geometry) run together: every iteration of
- * every problem is two persistent kernels pulling tiles of all problems from
- * one work queue, replayed as a CUDA graph.  The reference has no batch entry
- * point; it is the loop a user writes around siddon_recon::a0_RECON_MLEM
- * (hf_siddon_recon.hpp:91-108) over many scans.  Each problem's result is
- * bit-identical to recon_mlem on a plan of the same geometry and options.
- * EXACT arithmetic, Siddon back projector, FP32 sinograms only. */
+/* Many MLEM problems (each its own geometry) run together: one iteration of
+ * every problem is captured once as a CUDA graph whose parallel branches share
+ * the problems out (largest first), and replayed once per iteration.  The
+ * reference has no batch entry point; it is the loop a user writes around
+ * siddon_recon::a0_RECON_MLEM (hf_siddon_recon.hpp:91-108) over many scans.
+ * Each problem's result is bit-identical to recon_mlem on a plan of the same
+ * geometry and options.  EXACT arithmetic, Siddon back projector, FP32
+ * sinograms only. */
 typedef struct recon_batch* recon_batch_t;
 recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const recon_options_t* opt,
                                   recon_batch_t* batch);
 void recon_batch_destroy(recon_batch_t batch);
 /* d_g[p] / d_f[p]: problem p's sinogram [NumProj][Nv][Nu] and image
- * [Z][Y][X] on the batch's device.  The first call times a few candidate
- * launch shapes on the caller's data (the images are restored) and
- * synchronises; later calls are asynchronous on `stream`. */
+ * [Z][Y][X] on the batch's device.  The first call times graphs of 1, 2, 4
+ * and 8 branches on the caller's data (the images are restored) and
+ * synchronises; later calls are asynchronous on `stream` (a call with other
+ * buffers than the previous one captures the graph again). */
 recon_status_t recon_batch_mlem(recon_batch_t batch, const float* const* d_g, float* const* d_f,
                                 unsigned int iters, int init_ones, void* stream);
 
