@@ -167,31 +167,55 @@ __global__ void __launch_bounds__(128) bp_ray_kernel(ExactGeom G, const float4* 
     const int u = R.u, v = R.v;
     const unsigned view = R.view;
     if (u >= G.Nu || v >= G.Nv) return;
-    const int F = fix_exponent(*maxabs, max_len, count_bits);
-    if (F == INT_MIN) return;
     const size_t pix = (size_t)u + (size_t)v * G.Nu;
-    float val;
-    if (MODE == 1) val = __ldg(wtab + pix);
-    else val = load_val<ST>(sino + (size_t)(view - view0) * G.Nu * G.Nv + pix);
-    if (WEIGHTED && MODE != 1) val *= __ldg(wtab + pix);
-    if (val == 0.0f) return;
+    // every load the ray needs is issued before any is used
+    const unsigned mbits = __ldg(maxabs);
+    float val = (MODE == 1) ? __ldg(wtab + pix) : load_val<ST>(sino + (size_t)(view - view0) * G.Nu * G.Nv + pix);
+    const float wv = (WEIGHTED && MODE != 1) ? __ldg(wtab + pix) : 1.0f;
     const float2 C = __ldg(cs + view);
-    bp_ray_slab(G, __ldg(txy + (size_t)view * G.Nu + u), __ldg(kxy + (size_t)view * G.Nu + u), zp[v], k0, k1,
-                val * ldexpf(1.0f, F), fabsf(C.y) > fabsf(C.x), acc, acc_t);
+    const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+    const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+    const ZParam Z = zp[v];
+    const int F = fix_exponent(mbits, max_len, count_bits);
+    if (F == INT_MIN) return;
+    if (WEIGHTED && MODE != 1) val *= wv;
+    if (val == 0.0f) return;
+    bp_ray_slab(G, T, K, Z, k0, k1, val * ldexpf(1.0f, F), fabsf(C.y) > fabsf(C.x), acc, acc_t);
 }
 
-// Slab [k0, k1) of the result from the accumulators:
+// Slab [k0, k1) of the result from the accumulators, 32x32 (x, y) tiles of
+// one z slice per CTA of 32x8 threads (the transposed accumulator is read and
+// cleared through shared memory so that both are accessed coalesced):
 // MODE 0: vol = Ht; MODE 2: f = (sens != 0) ? f * Ht / sens : 0 (MLEM update).
 template <int MODE>
-__global__ void bp_finish_kernel(ExactGeom G, const unsigned* __restrict__ maxabs, float max_len, int count_bits,
-                                 int k0, int k1, unsigned long long* acc, unsigned long long* acc_t,
-                                 float* __restrict__ vol, const float* __restrict__ sens)
+__global__ void __launch_bounds__(256) bp_finish_kernel(ExactGeom G, const unsigned* __restrict__ maxabs,
+                                                         float max_len, int count_bits, int k0,
+                                                         unsigned long long* __restrict__ acc,
+                                                         unsigned long long* __restrict__ acc_t,
+                                                         float* __restrict__ vol, const float* __restrict__ sens)
 {
-    const int F = fix_exponent(*maxabs, max_len, count_bits);
-    const size_t plane = (size_t)G.X * G.Y, n = plane * (size_t)(k1 - k0);
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % G.X), y = (int)((i / G.X) % G.Y), zs = (int)(i / plane);
-        const float ht = bp_slab_value(G, x, y, zs, F, acc, acc_t);
+    __shared__ unsigned long long tile[32][33];
+    const int F = fix_exponent(__ldg(maxabs), max_len, count_bits);
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, zs = blockIdx.z;
+    const size_t plane = (size_t)G.X * G.Y, slab_off = (size_t)zs * plane;
+    for (int r = threadIdx.y; r < 32; r += 8) {  // acc_t[zs][x][y]: y along the warp
+        const int x = x0 + r, y = y0 + threadIdx.x;
+        unsigned long long q = 0ull;
+        if (x < G.X && y < G.Y) {
+            unsigned long long* p = acc_t + slab_off + (size_t)x * G.Y + y;
+            q = *p;
+            *p = 0ull;
+        }
+        tile[threadIdx.x][r] = q;  // [y - y0][x - x0]
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {  // acc[zs][y][x]: x along the warp
+        const int x = x0 + threadIdx.x, y = y0 + r;
+        if (x >= G.X || y >= G.Y) continue;
+        const size_t i = slab_off + (size_t)y * G.X + x;
+        const long long q = (long long)(acc[i] + tile[r][threadIdx.x]);
+        acc[i] = 0ull;
+        const float ht = (F != INT_MIN) ? (float)ldexp((double)q, -F) : 0.0f;
         const size_t vox = i + (size_t)k0 * plane;
         if (MODE == 2) {
             const float sv = sens[vox];
@@ -575,7 +599,6 @@ static recon_status_t launch_bp(Plan& P, const ST* sino, unsigned first, unsigne
     const int cbits = bp_count_bits(P, count);
     const int depth = bp_slab_depth(P);
     const dim3 blk = fp_block();
-    const unsigned fblocks = (unsigned)P.sm_count * 8;
     constexpr int RMODE = (MODE == 1) ? 1 : 0;
     const RayTiles none;
     for (int k0 = 0, slab = 0; k0 < P.eg.Z; k0 += depth, ++slab) {
@@ -592,8 +615,10 @@ static recon_status_t launch_bp(Plan& P, const ST* sino, unsigned first, unsigne
                                                                            P.d_bpacc_t);
             RB_CUDA(cudaGetLastError());
         }
-        exact::bp_finish_kernel<MODE == 2 ? 2 : 0><<<fblocks, 256, 0, s>>>(P.eg, P.d_bpmax, max_len, cbits, k0, k1,
-                                                                           P.d_bpacc, P.d_bpacc_t, vol, sens);
+        const dim3 fgrid((P.eg.X + 31) / 32, (P.eg.Y + 31) / 32, k1 - k0);
+        exact::bp_finish_kernel<MODE == 2 ? 2 : 0><<<fgrid, dim3(32, 8), 0, s>>>(P.eg, P.d_bpmax, max_len, cbits,
+                                                                                 k0, P.d_bpacc, P.d_bpacc_t, vol,
+                                                                                 sens);
         RB_CUDA(cudaGetLastError());
     }
     return RECON_OK;

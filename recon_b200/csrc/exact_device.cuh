@@ -232,18 +232,5 @@ __device__ __forceinline__ void bp_ray_slab(const ExactGeom& G, const float4 T, 
     }
 }
 
-// Fixed point -> float for voxel (x, y, z) of the slab starting at k0:
-// the sum of both accumulators, which are cleared for the next use.
-__device__ __forceinline__ float bp_slab_value(const ExactGeom& G, int x, int y, int zs, int F,
-                                               unsigned long long* acc, unsigned long long* acc_t)
-{
-    const size_t a = (size_t)x + (size_t)y * G.X + (size_t)zs * G.X * G.Y;
-    const size_t b = (size_t)y + (size_t)x * G.Y + (size_t)zs * G.X * G.Y;
-    const long long q = (long long)(acc[a] + acc_t[b]);
-    acc[a] = 0ull;
-    acc_t[b] = 0ull;
-    return (F != INT_MIN) ? (float)ldexp((double)q, -F) : 0.0f;
-}
-
 }  // namespace exact
 }  // namespace rb
