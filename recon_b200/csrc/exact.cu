@@ -195,34 +195,45 @@ __global__ void __launch_bounds__(256) bp_finish_kernel(ExactGeom G, const unsig
                                                          float* __restrict__ vol, const float* __restrict__ sens)
 {
     __shared__ unsigned long long tile[32][33];
-    const int F = fix_exponent(__ldg(maxabs), max_len, count_bits);
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, zs = blockIdx.z;
     const size_t plane = (size_t)G.X * G.Y, slab_off = (size_t)zs * plane;
-    for (int r = threadIdx.y; r < 32; r += 8) {  // acc_t[zs][x][y]: y along the warp
-        const int x = x0 + r, y = y0 + threadIdx.x;
-        unsigned long long q = 0ull;
-        if (x < G.X && y < G.Y) {
-            unsigned long long* p = acc_t + slab_off + (size_t)x * G.Y + y;
-            q = *p;
-            *p = 0ull;
-        }
-        tile[threadIdx.x][r] = q;  // [y - y0][x - x0]
+    // all loads first: the transposed accumulator (y along the warp), then
+    // this thread's accumulator, sensitivity and image values (x along the warp)
+    unsigned long long qt[4], qa[4];
+    float sv[4], fv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int x = x0 + threadIdx.y + 8 * r, y = y0 + threadIdx.x;
+        qt[r] = (x < G.X && y < G.Y) ? acc_t[slab_off + (size_t)x * G.Y + y] : 0ull;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int x = x0 + threadIdx.x, y = y0 + threadIdx.y + 8 * r;
+        const bool in = x < G.X && y < G.Y;
+        const size_t i = slab_off + (size_t)y * G.X + x;
+        qa[r] = in ? acc[i] : 0ull;
+        sv[r] = (MODE == 2 && in) ? sens[i + (size_t)k0 * plane] : 0.0f;
+        fv[r] = (MODE == 2 && in) ? vol[i + (size_t)k0 * plane] : 0.0f;
+    }
+    const int F = fix_exponent(__ldg(maxabs), max_len, count_bits);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int x = x0 + threadIdx.y + 8 * r, y = y0 + threadIdx.x;
+        tile[threadIdx.x][threadIdx.y + 8 * r] = qt[r];  // [y - y0][x - x0]
+        if (x < G.X && y < G.Y) acc_t[slab_off + (size_t)x * G.Y + y] = 0ull;
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += 8) {  // acc[zs][y][x]: x along the warp
-        const int x = x0 + threadIdx.x, y = y0 + r;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int x = x0 + threadIdx.x, y = y0 + threadIdx.y + 8 * r;
         if (x >= G.X || y >= G.Y) continue;
         const size_t i = slab_off + (size_t)y * G.X + x;
-        const long long q = (long long)(acc[i] + tile[r][threadIdx.x]);
+        const long long q = (long long)(qa[r] + tile[threadIdx.y + 8 * r][threadIdx.x]);
         acc[i] = 0ull;
         const float ht = (F != INT_MIN) ? (float)ldexp((double)q, -F) : 0.0f;
         const size_t vox = i + (size_t)k0 * plane;
-        if (MODE == 2) {
-            const float sv = sens[vox];
-            vol[vox] = (sv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[vox], ht), sv) : 0.0f;
-        } else {
-            vol[vox] = ht;
-        }
+        if (MODE == 2) vol[vox] = (sv[r] != 0.0f) ? __fdiv_rn(__fmul_rn(fv[r], ht), sv[r]) : 0.0f;
+        else vol[vox] = ht;
     }
 }
 
