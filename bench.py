@@ -42,6 +42,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="recon_b200", choices=["recon_b200", "reference"])
     ap.add_argument("--sum", default="kahan", choices=["kahan", "plain"])
+    ap.add_argument("--sino", default="f32", choices=["f32", "bf16"],
+                    help="storage of the measured and ratio sinograms (FP32 accumulation either way)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-steps", type=int, default=24)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain leg")
@@ -133,6 +135,22 @@ def make_problem(cfg, device):
     g = noisy(p, cfg["I0"], cfg["seed"])
     del p
     return vol, g
+
+
+TRAFFIC_PROFILE = "profiles/exact_fp_bp_plain256_360v_512.md"
+
+
+def measured_traffic() -> dict:
+    """DRAM bytes per forward / back projection of the bench workload, from the
+    committed ncu summary (line `traffic-per-launch: fp=<bytes> bp=<bytes>`)."""
+    import re
+
+    try:
+        text = open(os.path.join(ROOT, TRAFFIC_PROFILE)).read()
+    except OSError:
+        return {}
+    m = re.search(r"traffic-per-launch:\s*fp=(\d+)\s+bp=(\d+)", text)
+    return {"fp": int(m.group(1)), "bp": int(m.group(2))} if m else {}
 
 
 def batched_leg(device, n_prob: int, iters: int, opts):
@@ -294,7 +312,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from recon_b200 import SUM_KAHAN, SUM_PLAIN, Options, Plan
+    from recon_b200 import SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN, Options, Plan
     from recon_b200.configs import PLAIN_GPU
     from recon_b200.sharding import ordered_sum_, view_range
 
@@ -316,8 +334,11 @@ def main():
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     cfg = dict(PLAIN_GPU)
-    opts = Options(sum=SUM_KAHAN if args.sum == "kahan" else SUM_PLAIN, device=local)
+    opts = Options(sum=SUM_KAHAN if args.sum == "kahan" else SUM_PLAIN,
+                   sino=SINO_BF16 if args.sino == "bf16" else SINO_F32, device=local)
     vol, g = make_problem(cfg, device)
+    if args.sino == "bf16":
+        g = g.to(torch.bfloat16)
     P = Plan(cfg, opts)
     nviews = int(cfg["NumProj"])
     isects = P.count_intersections()
@@ -327,6 +348,12 @@ def main():
     first, count = view_range(nviews, rank, world)
     npix = P.nu * P.nv
     nvox = f.numel()
+    # z-slabs of the back projector (librecon_b200: both int64 accumulators of a
+    # slab in 64 MiB); per step: transpose + forward, maxabs + (ray + finish) per
+    # slab, and at N > 1 a separate update
+    Z, Y, X = P.shape_vol
+    depth = max(1, min(Z, (64 << 20) // (X * Y * 16)))
+    slabs = -(-Z // depth)
 
     def iteration(ev=None):
         if world == 1:
@@ -400,15 +427,15 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32" if args.sino == "f32" else "f32 (bf16 sinograms)",
         "data": "synthetic (seeded 40-ellipsoid phantom in a 0.02/mm cylinder, Poisson noise I0=1e5)",
         "config": {"workload": WORKLOAD, "volume": [256, 256, 256], "voxel_mm": 0.25, "views": nviews,
                    "detector": [512, 512], "pixel_mm": 0.5, "arith": "exact",
-                   "sum": args.sum, "parallelism": f"views/{world}" if world > 1 else "single",
+                   "sum": args.sum, "sino": args.sino, "parallelism": f"views/{world}" if world > 1 else "single",
                    "l2": "no flush: per-step inputs (377 MB sinogram + 377 MB ratio) exceed the 126 MB L2"},
         "isects_per_pass": isects,
         "isects_per_s": 2.0 * isects * value,
-        "gpu_launches": 2 * args.steps if world == 1 else 3 * args.steps,
+        "gpu_launches": args.steps * (3 + 2 * slabs if world == 1 else 4 + 2 * slabs),
     }
     peaks = {}
     try:
@@ -422,10 +449,16 @@ def main():
         t_bp = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
         bytes_fp = 4.0 * isects + 4.0 * npix * nviews
         bytes_bp = 4.0 * isects + 12.0 * nvox
-        dom = ("bp_gather", t_bp, bytes_bp) if t_bp >= t_fp else ("fp_ratio", t_fp, bytes_fp)
+        traffic = measured_traffic()
+        if t_bp >= t_fp:
+            dom = ("back projection (maxabs + bp_ray_kernel per z-slab + bp_finish_kernel)", t_bp, bytes_bp,
+                   traffic.get("bp"))
+        else:
+            dom = ("forward projection (transpose_xy_kernel + fp_kernel)", t_fp, bytes_fp, traffic.get("fp"))
         ach = dom[2] / (dom[1] * 1e-3) / 1e9
         out["roofline"] = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": hbm, "unit": "GB/s",
-                           "frac": ach / hbm, "peak_source": peak_src, "traffic": None,
+                           "frac": ach / hbm, "peak_source": peak_src, "traffic": dom[3],
+                           "traffic_source": TRAFFIC_PROFILE if dom[3] is not None else None,
                            "algorithmic_bytes_per_launch": dom[2], "launch_ms": dom[1]}
         b_iter = 8.0 * isects + 4.0 * npix * nviews + 12.0 * nvox
         out["iteration_roofline"] = {"bytes_per_iteration": b_iter, "achieved_gbs": b_iter / (ms_step * 1e-3) / 1e9,
