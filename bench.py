@@ -49,6 +49,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain leg")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched-vs-plain leg and print it as the JSON line")
+    ap.add_argument("--no-voxel", action="store_true", help="skip the voxel-driven back projector leg")
     ap.add_argument("--batched-problems", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=20)
     return ap.parse_args()
@@ -202,6 +203,32 @@ def batched_leg(device, n_prob: int, iters: int, opts):
                    "views_min_max": [min(int(c["NumProj"]) for c in cfgs), max(int(c["NumProj"]) for c in cfgs)],
                    "isects_per_pass": isects},
     }
+
+
+def voxel_leg(cfg, g, steps: int, warmup: int, device_index: int):
+    """The same MLEM iteration with the voxel-driven back projector
+    (texture point fetches + FP32 bilinear weights, geometric mode) in place
+    of the Siddon one: Siddon forward projection with the plain ratio, then
+    the voxel-driven back projection with the update fused in."""
+    import torch
+
+    from recon_b200 import BP_VOXEL, VOXEL_GEOMETRIC, Options, Plan
+
+    P = Plan(cfg, Options(bp=BP_VOXEL, voxel_mode=VOXEL_GEOMETRIC, device=device_index))
+    P.mlem_prepare()
+    f = P.new_volume(1.0)
+    for _ in range(warmup):
+        P.mlem_iteration(g, f)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(steps):
+        P.mlem_iteration(g, f)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    return {"value": 1e3 / ms, "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
+            "back_projector": "voxel-driven, texture point fetch + FP32 bilinear (geometric mode)"}
 
 
 def ref_view_seconds(R, O, geo, cfg, view, steps, f, gview, ht):
@@ -472,8 +499,12 @@ def main():
                                                args.cpu_baseline_steps)
         except Exception as e:  # pragma: no cover
             out["cpu_baseline"] = {"error": str(e)}
+    if world == 1 and not args.no_voxel and args.sino == "f32":
+        del P
+        torch.cuda.empty_cache()
+        out["voxel_bp"] = voxel_leg(cfg, g, max(3, args.steps // 4), args.warmup, local)
     if world == 1 and not args.no_batched:
-        del g_host, f_host, g, vol, P
+        del g_host, f_host, g, vol
         torch.cuda.empty_cache()
         out["batched"] = batched_leg(device, args.batched_problems, args.batched_iters, opts)
     print(json.dumps(out))

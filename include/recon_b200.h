@@ -223,6 +223,19 @@ recon_status_t recon_mlem_update(recon_plan_t plan, float* d_f, const float* d_h
  * recon_mlem_forward(all views) followed by this is one recon_mlem_iteration. */
 recon_status_t recon_mlem_backward_update(recon_plan_t plan, float* d_f, void* stream);
 
+/* OSEM (ordered-subset EM) from d_f (or f = 1 with init_ones): `iters` full
+ * passes over n_subsets contiguous subsets of NumProj / n_subsets views each;
+ * per subset s, f <- f * BP_s(g / FP_s(f)) / BP_s(1) with MLEM's zero guards.
+ * The reference stops at the parameter structs osem_input_values /
+ * osem_subset_inputs and their check check_recon_inputs
+ * (hf_cpp_functions.hpp:298-375): n_subsets must divide NumProj
+ * (RECON_ERR_INVALID_ARGUMENT otherwise) and a subset is a contiguous arc of
+ * views.  With n_subsets = 1 this is recon_mlem, bit for bit.  EXACT
+ * arithmetic, Siddon back projector; the per-subset sensitivities are
+ * computed on the first call for a subset count and cached in the plan. */
+recon_status_t recon_osem(recon_plan_t plan, const void* d_g, unsigned int iters, unsigned int n_subsets,
+                          float* d_f, int init_ones, void* stream);
+
 /* ---- batches of independent reconstructions ------------------------------ */
 
 /* Many MLEM problems (each its own geometry) run together: one iteration of

@@ -91,6 +91,8 @@ def lib():
         L.orc_x_fp_all.argtypes = [_GP, C.c_uint, C.c_float, _f64p, _f64p, C.c_int]
         L.orc_x_bp_all.argtypes = [_GP, C.c_uint, C.c_float, _f64p, _f64p, C.c_int]
         L.orc_x_mlem.argtypes = [_GP, C.c_uint, C.c_float, _f32p, C.c_uint, _f64p, C.c_void_p, C.c_int]
+        L.orc_x_osem.argtypes = [_GP, C.c_uint, C.c_float, _f32p, C.c_uint, C.c_uint, _f64p, C.c_int]
+        L.orc_x_osem.restype = C.c_int
         L.orc_x_count_isects.argtypes = [_GP, C.c_uint, C.c_float, C.c_int]
         L.orc_x_count_isects.restype = C.c_int64
         L.orc_x_voxel_column.argtypes = [_GP, C.c_uint, C.c_float, C.c_int64, _i32p, _i32p, _f64p, C.c_int]
@@ -255,6 +257,16 @@ def x_mlem(g: Geom, nproj: int, dang: float, sino: np.ndarray, iters: int, threa
     lib().orc_x_mlem(C.byref(g), nproj, dang, np.ascontiguousarray(sino, np.float32).ravel(), iters, f,
                      sens.ctypes.data_as(C.c_void_p), threads)
     return f, sens
+
+
+def x_osem(g: Geom, nproj: int, dang: float, sino: np.ndarray, iters: int, subsets: int, threads: int = 0):
+    """FP64 OSEM, contiguous subsets (orc_x_osem)."""
+    f = np.zeros(g.nvox, np.float64)
+    rc = lib().orc_x_osem(C.byref(g), nproj, dang, np.ascontiguousarray(sino, np.float32).ravel(), iters, subsets,
+                          f, threads)
+    if rc != 0:
+        raise ValueError(f"{subsets} subsets do not divide {nproj} views")
+    return f
 
 
 def x_count_isects(g: Geom, nproj: int, dang: float, threads: int = 0) -> int:

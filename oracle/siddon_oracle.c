@@ -795,15 +795,23 @@ static int set_threads(int threads)
 #endif
 }
 
-void orc_x_fp_all(const orc_geom* g, unsigned int NumProj, float DeltaAng, const double* vol,
-                  double* sino, int threads)
+/* Views first .. first+count-1 (view n at (float)n * DeltaAng) into sino
+ * (count images back to back). */
+static void x_fp_views(const orc_geom* g, unsigned int first, unsigned int count, float DeltaAng,
+                       const double* vol, double* sino, int threads)
 {
     const size_t Npix = (size_t)g->NumAxPixels * g->NumTAxPixels;
     int nt = set_threads(threads);
     (void)nt;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
-    for (long n = 0; n < (long)NumProj; ++n)
-        orc_x_fp_view(g, (float)n * DeltaAng, vol, sino + (size_t)n * Npix);
+    for (long n = 0; n < (long)count; ++n)
+        orc_x_fp_view(g, (float)(first + (unsigned)n) * DeltaAng, vol, sino + (size_t)n * Npix);
+}
+
+void orc_x_fp_all(const orc_geom* g, unsigned int NumProj, float DeltaAng, const double* vol,
+                  double* sino, int threads)
+{
+    x_fp_views(g, 0, NumProj, DeltaAng, vol, sino, threads);
 }
 
 typedef struct {
@@ -819,8 +827,18 @@ static void x_emit_bp(void* c, int64_t vox, double len)
 /* Ray-driven FP64 back projection, deterministic for a given thread count:
  * views are split statically over threads, each thread owns a partial
  * volume, partials are summed in thread order. */
+static void x_bp_views(const orc_geom* g, unsigned int first, unsigned int NumProj, float DeltaAng,
+                       const double* sino, double* vol, int threads);
+
 void orc_x_bp_all(const orc_geom* g, unsigned int NumProj, float DeltaAng, const double* sino,
                   double* vol, int threads)
+{
+    x_bp_views(g, 0, NumProj, DeltaAng, sino, vol, threads);
+}
+
+/* Views first .. first+NumProj-1 of sino (NumProj images back to back). */
+static void x_bp_views(const orc_geom* g, unsigned int first, unsigned int NumProj, float DeltaAng,
+                       const double* sino, double* vol, int threads)
 {
     const unsigned Nu = g->NumAxPixels, Nv = g->NumTAxPixels;
     const size_t Npix = (size_t)Nu * Nv;
@@ -837,7 +855,7 @@ void orc_x_bp_all(const orc_geom* g, unsigned int NumProj, float DeltaAng, const
 #endif
         double* pv = part + (size_t)t * V;
         for (unsigned n = (unsigned)t; n < NumProj; n += (unsigned)nt) {
-            float ang = (float)n * DeltaAng;
+            float ang = (float)(first + n) * DeltaAng;
             const double* img = sino + (size_t)n * Npix;
             for (unsigned v = 0; v < Nv; ++v)
                 for (unsigned u = 0; u < Nu; ++u) {
@@ -880,6 +898,40 @@ void orc_x_mlem(const orc_geom* g, unsigned int NumProj, float DeltaAng, const f
     free(sino);
     free(Ht);
     if (!sens_out) free(sens);
+}
+
+/* OSEM in FP64 with N_subsets contiguous subsets of NumProj / N_subsets
+ * views (the subset layout of osem_input_values / check_recon_inputs,
+ * hf_cpp_functions.hpp:298-375, where the reference stops): per subset s,
+ * f <- f * BP_s(g / FP_s(f)) / BP_s(1) with the zero guards of MLEM.
+ * Returns 0, or -1 when N_subsets does not divide NumProj. */
+int orc_x_osem(const orc_geom* g, unsigned int NumProj, float DeltaAng, const float* g_sino, unsigned int iters,
+               unsigned int N_subsets, double* f, int threads)
+{
+    if (N_subsets == 0 || NumProj % N_subsets != 0) return -1;
+    const unsigned n = NumProj / N_subsets;
+    const size_t Npix = (size_t)g->NumAxPixels * g->NumTAxPixels;
+    const size_t Ps = Npix * n;
+    const size_t V = (size_t)g->Xdim * g->Ydim * g->Zdim;
+    double* sino = (double*)malloc(Ps * sizeof(double));
+    double* Ht = (double*)malloc(V * sizeof(double));
+    double* sens = (double*)malloc((size_t)N_subsets * V * sizeof(double));
+    for (size_t i = 0; i < Ps; ++i) sino[i] = 1.0;
+    for (unsigned s = 0; s < N_subsets; ++s) x_bp_views(g, s * n, n, DeltaAng, sino, sens + (size_t)s * V, threads);
+    for (size_t i = 0; i < V; ++i) f[i] = 1.0;
+    for (unsigned it = 0; it < iters; ++it)
+        for (unsigned s = 0; s < N_subsets; ++s) {
+            const double* ss = sens + (size_t)s * V;
+            const float* gs = g_sino + (size_t)s * Ps;
+            x_fp_views(g, s * n, n, DeltaAng, f, sino, threads);
+            for (size_t i = 0; i < Ps; ++i) sino[i] = (sino[i] != 0.0) ? (double)gs[i] / sino[i] : 0.0;
+            x_bp_views(g, s * n, n, DeltaAng, sino, Ht, threads);
+            for (size_t i = 0; i < V; ++i) f[i] = (ss[i] != 0.0) ? f[i] * Ht[i] / ss[i] : 0.0;
+        }
+    free(sino);
+    free(Ht);
+    free(sens);
+    return 0;
 }
 
 typedef struct {

@@ -177,6 +177,13 @@ class Plan:
         check(lib().recon_mlem(self._h, _ptr(g), int(iters), _ptr(f), 1 if init_ones else 0, _stream()))
         return f
 
+    def osem(self, g, iters: int, subsets: int, f=None, init_ones: bool = True):
+        """recon_osem: `iters` passes over `subsets` contiguous view subsets."""
+        f = self.new_volume() if f is None else f
+        check(lib().recon_osem(self._h, _ptr(g), int(iters), int(subsets), _ptr(f), 1 if init_ones else 0,
+                               _stream()))
+        return f
+
     def mlem_prepare(self) -> None:
         check(lib().recon_mlem_prepare(self._h, _stream()))
 

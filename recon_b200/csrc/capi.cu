@@ -1,5 +1,6 @@
 // capi.cu -- the C ABI (include/recon_b200.h): plans, projectors, MLEM,
 // elementwise drop-ins and the parity entry points.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -452,6 +453,49 @@ recon_status_t recon_mlem_backward_update(recon_plan_t P, float* d_f, void* stre
     RB_CHECK(use_device(*P));
     return exact_bp(*P, P->d_ratio, true, P->opt.sino == RECON_SINO_BF16, 0, P->nviews, false, false, nullptr,
                     P->d_sens, d_f, as_stream(stream));
+}
+
+recon_status_t recon_osem(recon_plan_t P, const void* d_g, unsigned iters, unsigned n_subsets, float* d_f,
+                          int init_ones, void* stream)
+{
+    if (!P || !d_g || !d_f) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (P->opt.arith != RECON_ARITH_EXACT || P->opt.bp != RECON_BP_SIDDON)
+        return fail(RECON_ERR_UNSUPPORTED, "OSEM needs EXACT arithmetic and the Siddon back projector");
+    // check_recon_inputs (hf_cpp_functions.hpp:358-375): the subsets must split the views evenly
+    if (n_subsets == 0 || P->nviews == 0 || P->nviews % n_subsets != 0)
+        return fail(RECON_ERR_INVALID_ARGUMENT, "The input values does not agree with each other: "
+                                                "N_subsets must divide NumProj");
+    RB_CHECK(use_device(*P));
+    cudaStream_t s = as_stream(stream);
+    RB_CHECK(ensure_mlem_buffers(*P));
+    const unsigned n = P->nviews / n_subsets;
+    if (P->osem_subsets != n_subsets) {
+        // per-subset sensitivities BP_s(1), computed once per subset count
+        if (P->d_osem_sens) {
+            cudaFree(P->d_osem_sens);
+            P->allocations.erase(std::find(P->allocations.begin(), P->allocations.end(), (void*)P->d_osem_sens));
+            P->device_bytes -= (size_t)P->osem_subsets * P->nvox * sizeof(float);
+            P->d_osem_sens = nullptr;
+            P->osem_subsets = 0;
+        }
+        RB_CHECK(P->alloc(&P->d_osem_sens, (size_t)n_subsets * P->nvox, "OSEM subset sensitivities"));
+        for (unsigned k = 0; k < n_subsets; ++k)
+            RB_CHECK(exact_bp(*P, nullptr, false, false, k * n, n, false, true, P->d_osem_sens + (size_t)k * P->nvox,
+                              nullptr, nullptr, s));
+        P->osem_subsets = n_subsets;
+    }
+    if (init_ones) RB_CHECK(launch_fill(d_f, 1.0f, P->nvox, s));
+    const bool bf16 = P->opt.sino == RECON_SINO_BF16;
+    const size_t es = bf16 ? 2 : 4;
+    for (unsigned it = 0; it < iters; ++it)
+        for (unsigned k = 0; k < n_subsets; ++k) {
+            const unsigned first = k * n;
+            RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, s, first, n));
+            const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * P->npix * es;
+            RB_CHECK(exact_bp(*P, r, true, bf16, first, n, false, false, nullptr,
+                              P->d_osem_sens + (size_t)k * P->nvox, d_f, s));
+        }
+    return RECON_OK;
 }
 
 recon_status_t recon_view_step_count(recon_plan_t P, float angle, unsigned* loopN)

@@ -118,6 +118,8 @@ struct Plan {
     unsigned* d_loopN = nullptr;  // [view] (+1 scratch slot)
     // workspaces
     float* d_sens = nullptr;      // cached sensitivity
+    float* d_osem_sens = nullptr; // OSEM: per-subset sensitivities [osem_subsets][nvox]
+    unsigned osem_subsets = 0;
     bool sens_valid = false;
     void* d_ratio = nullptr;      // ratio sinogram (float or bf16) [nviews][npix]
     float* d_ht = nullptr;        // COMPAT: Ht accumulator [nvox]

@@ -193,3 +193,18 @@ def test_compat_vs_fp64_close():
         O.lib().orc_x_fp_view(g, ang, vol.astype(np.float64), x)
         err = np.linalg.norm(c - x) / np.linalg.norm(x)
         assert err < 5e-2, err
+
+
+def test_fp64_osem_one_subset_is_mlem_and_checks_subsets():
+    # OSEM of the oracle (contiguous subsets, osem_input_values / check_recon_inputs,
+    # hf_cpp_functions.hpp:298-375): one subset is MLEM exactly; a subset count
+    # that does not divide the views is refused
+    cfg = small_cfg(Xdim=12, Ydim=12, Zdim=8, AxPixels=20, TAxPixels=16, AxPixDim=2.0, TAxPixDim=2.0, NumProj=6)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    sino = np.random.default_rng(5).random(6 * g.npix).astype(np.float32)
+    f_mlem, _ = O.x_mlem(g, 6, np.float32(60.0), sino, 2)
+    assert np.array_equal(O.x_osem(g, 6, np.float32(60.0), sino, 2, 1), f_mlem)
+    f3 = O.x_osem(g, 6, np.float32(60.0), sino, 2, 3)
+    assert np.all(np.isfinite(f3)) and not np.array_equal(f3, f_mlem)
+    with pytest.raises(ValueError):
+        O.x_osem(g, 6, np.float32(60.0), sino, 1, 4)
