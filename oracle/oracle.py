@@ -93,6 +93,8 @@ def lib():
         L.orc_x_mlem.argtypes = [_GP, C.c_uint, C.c_float, _f32p, C.c_uint, _f64p, C.c_void_p, C.c_int]
         L.orc_x_osem.argtypes = [_GP, C.c_uint, C.c_float, _f32p, C.c_uint, C.c_uint, _f64p, C.c_int]
         L.orc_x_osem.restype = C.c_int
+        L.orc_x_slab_update.argtypes = [_GP, C.c_uint, C.c_float, _f32p, _f32p, C.c_uint, C.c_uint, _f64p, C.c_int]
+        L.orc_x_slab_update.restype = C.c_int
         L.orc_x_count_isects.argtypes = [_GP, C.c_uint, C.c_float, C.c_int]
         L.orc_x_count_isects.restype = C.c_int64
         L.orc_x_voxel_column.argtypes = [_GP, C.c_uint, C.c_float, C.c_int64, _i32p, _i32p, _f64p, C.c_int]
@@ -267,6 +269,17 @@ def x_osem(g: Geom, nproj: int, dang: float, sino: np.ndarray, iters: int, subse
     if rc != 0:
         raise ValueError(f"{subsets} subsets do not divide {nproj} views")
     return f
+
+
+def x_slab_update(g: Geom, nproj: int, dang: float, f: np.ndarray, sino: np.ndarray, z0: int, z1: int,
+                  threads: int = 0) -> np.ndarray:
+    """FP64 MLEM update of the slab z in [z0, z1) from an FP32 image (orc_x_slab_update)."""
+    out = np.zeros((z1 - z0) * g.Xdim * g.Ydim, np.float64)
+    rc = lib().orc_x_slab_update(C.byref(g), nproj, dang, np.ascontiguousarray(f, np.float32).ravel(),
+                                 np.ascontiguousarray(sino, np.float32).ravel(), z0, z1, out, threads)
+    if rc != 0:
+        raise ValueError("bad slab or out of memory")
+    return out
 
 
 def x_count_isects(g: Geom, nproj: int, dang: float, threads: int = 0) -> int:

@@ -934,6 +934,97 @@ int orc_x_osem(const orc_geom* g, unsigned int NumProj, float DeltaAng, const fl
     return 0;
 }
 
+/* One MLEM update of the slab z in [z0, z1) of a large volume, in FP64, from
+ * an FP32 image f and FP32 data: for every ray that crosses the slab, its full
+ * line integral Hf through f, the ratio g/Hf (0 where Hf = 0) and the back
+ * projection of the ratio and of 1 into the slab's voxels; then
+ * out = f * Ht / sens over the slab (0 where sens = 0) -- the update of
+ * hf_siddon_recon.hpp:437-476 for the slab, with the sensitivity of all
+ * views.  Views are split over threads, each with its own slab partials,
+ * summed in thread order.  Returns 0, or -1 on a bad slab or allocation
+ * failure. */
+typedef struct {
+    const float* f;
+    double sum;
+    int64_t lo, hi;  /* slab voxel range [lo, hi) */
+    int64_t* idx;
+    double* len;
+    int n;
+} x_slab_ctx;
+static void x_emit_slab(void* c, int64_t vox, double len)
+{
+    x_slab_ctx* t = (x_slab_ctx*)c;
+    t->sum += len * (double)t->f[vox];
+    if (vox >= t->lo && vox < t->hi) {
+        t->idx[t->n] = vox - t->lo;
+        t->len[t->n] = len;
+        t->n++;
+    }
+}
+
+int orc_x_slab_update(const orc_geom* g, unsigned int NumProj, float DeltaAng, const float* f,
+                      const float* g_meas, unsigned int z0, unsigned int z1, double* out, int threads)
+{
+    if (z0 >= z1 || z1 > g->Zdim) return -1;
+    const unsigned Nu = g->NumAxPixels, Nv = g->NumTAxPixels;
+    const size_t Npix = (size_t)Nu * Nv;
+    const size_t plane = (size_t)g->Xdim * g->Ydim;
+    const size_t S = plane * (z1 - z0);
+    const int64_t lo = (int64_t)(plane * z0), hi = (int64_t)(plane * z1);
+    const double zlo = -(double)g->Zdim / 2.0 * g->ZVoxSize + z0 * (double)g->ZVoxSize;
+    const double zhi = -(double)g->Zdim / 2.0 * g->ZVoxSize + z1 * (double)g->ZVoxSize;
+    int nt = set_threads(threads);
+    if ((unsigned)nt > NumProj) nt = (int)NumProj;
+    if (nt < 1) nt = 1;
+    double* part = (double*)calloc((size_t)nt * 2 * S, sizeof(double));
+    if (!part) return -1;
+    const int cap = (int)(g->Xdim + g->Ydim + g->Zdim + 4);
+#pragma omp parallel num_threads(nt)
+    {
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        double* ht = part + (size_t)t * 2 * S;
+        double* sn = ht + S;
+        int64_t* idx = (int64_t*)malloc((size_t)cap * sizeof(int64_t));
+        double* len = (double*)malloc((size_t)cap * sizeof(double));
+        for (unsigned n = (unsigned)t; n < NumProj; n += (unsigned)nt) {
+            const float ang = (float)n * DeltaAng;
+            for (unsigned v = 0; v < Nv; ++v)
+                for (unsigned u = 0; u < Nu; ++u) {
+                    orc_x_ray r;
+                    orc_x_ray_geom(g, ang, (int)u, (int)v, &r);
+                    /* the ray's z over its length: skip rays that never reach the slab */
+                    const double za = r.p1[2] < r.p2[2] ? r.p1[2] : r.p2[2];
+                    const double zb = r.p1[2] < r.p2[2] ? r.p2[2] : r.p1[2];
+                    if (zb < zlo || za > zhi) continue;
+                    x_slab_ctx c = {f, 0.0, lo, hi, idx, len, 0};
+                    x_traverse(g, &r, x_emit_slab, &c);
+                    if (c.n == 0) continue;
+                    const double gm = (double)g_meas[(size_t)n * Npix + u + (size_t)v * Nu];
+                    const double ratio = (c.sum != 0.0) ? gm / c.sum : 0.0;
+                    for (int k = 0; k < c.n; ++k) {
+                        ht[c.idx[k]] += c.len[k] * ratio;
+                        sn[c.idx[k]] += c.len[k];
+                    }
+                }
+        }
+        free(idx);
+        free(len);
+    }
+    for (size_t i = 0; i < S; ++i) {
+        double h = 0.0, s = 0.0;
+        for (int t = 0; t < nt; ++t) {
+            h += part[(size_t)t * 2 * S + i];
+            s += part[(size_t)t * 2 * S + S + i];
+        }
+        out[i] = (s != 0.0) ? (double)f[lo + (int64_t)i] * h / s : 0.0;
+    }
+    free(part);
+    return 0;
+}
+
 typedef struct {
     int64_t n;
 } x_count_ctx;

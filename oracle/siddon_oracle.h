@@ -101,6 +101,8 @@ void orc_x_mlem(const orc_geom* g, unsigned int NumProj, float DeltaAng, const f
                 unsigned int iters, double* f, double* sens_out, int threads);
 int orc_x_osem(const orc_geom* g, unsigned int NumProj, float DeltaAng, const float* g_sino, unsigned int iters,
                unsigned int N_subsets, double* f, int threads);
+int orc_x_slab_update(const orc_geom* g, unsigned int NumProj, float DeltaAng, const float* f,
+                      const float* g_meas, unsigned int z0, unsigned int z1, double* out, int threads);
 int64_t orc_x_count_isects(const orc_geom* g, unsigned int NumProj, float DeltaAng, int threads);
 /* column of the system matrix for one voxel: every (view, pixel, length) */
 int orc_x_voxel_column(const orc_geom* g, unsigned int NumProj, float DeltaAng, int64_t voxel,

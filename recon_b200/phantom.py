@@ -30,8 +30,12 @@ def _centers(n: int, vox: float) -> np.ndarray:
 
 
 def phantom(cfg: dict, seed: int | None = None, n_ellipsoids: int | None = None,
-            n_inserts: int | None = None) -> np.ndarray:
-    """Attenuation volume (float32, shape (Zdim, Ydim, Xdim)) for a preset dict."""
+            n_inserts: int | None = None, device=None):
+    """Attenuation volume (float32, shape (Zdim, Ydim, Xdim)) for a preset dict.
+
+    With ``device`` (a torch device) the voxelisation runs there and a torch
+    tensor is returned; the random draws are the same numpy ones, so only the
+    arithmetic's platform differs."""
     seed = cfg.get("seed", 0) if seed is None else seed
     n_ell = cfg.get("n_ellipsoids", 10) if n_ellipsoids is None else n_ellipsoids
     n_ins = cfg.get("n_inserts", 0) if n_inserts is None else n_inserts
@@ -39,6 +43,8 @@ def phantom(cfg: dict, seed: int | None = None, n_ellipsoids: int | None = None,
     vx, vy, vz = float(cfg["XVoxSize"]), float(cfg["YVoxSize"]), float(cfg["ZVoxSize"])
     rng = np.random.default_rng(seed)
     xs, ys, zs = _centers(X, vx), _centers(Y, vy), _centers(Z, vz)
+    if device is not None:
+        return _phantom_torch(rng, xs, ys, zs, X, Y, Z, vx, vy, vz, n_ell, n_ins, device)
     ext_xy = min(X * vx, Y * vy)
     scale = max(X * vx, Y * vy, Z * vz) / 32.0
     rcyl = 0.45 * ext_xy
@@ -61,6 +67,48 @@ def phantom(cfg: dict, seed: int | None = None, n_ellipsoids: int | None = None,
         q = (A[0, 0] * px * px + A[1, 1] * py * py + A[2, 2] * pz * pz +
              2.0 * (A[0, 1] * px * py + A[0, 2] * px * pz + A[1, 2] * py * pz))
         vol[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] += np.float32(value) * (q <= 1.0)
+
+    for _ in range(n_ell):
+        axes = rng.uniform(2.0, 12.0, size=3) * scale
+        rho = rcyl * np.sqrt(rng.uniform())
+        phi = rng.uniform(0.0, 2 * np.pi)
+        center = np.array([rho * np.cos(phi), rho * np.sin(phi), rng.uniform(-0.8, 0.8) * zhalf])
+        add_blob(center, axes, _random_rotation(rng), rng.uniform(0.01, 0.05))
+    for _ in range(n_ins):
+        rad = rng.uniform(1.0, 3.0) * scale
+        rho = (rcyl - rad) * np.sqrt(rng.uniform())
+        phi = rng.uniform(0.0, 2 * np.pi)
+        center = np.array([rho * np.cos(phi), rho * np.sin(phi), rng.uniform(-0.6, 0.6) * zhalf])
+        add_blob(center, np.array([rad, rad, rad]), np.eye(3), 0.2)
+    return vol
+
+
+def _phantom_torch(rng, xs, ys, zs, X, Y, Z, vx, vy, vz, n_ell, n_ins, device):
+    """phantom() voxelised with torch on `device` (same draws, same rule)."""
+    import torch
+
+    tx, ty, tz = (torch.as_tensor(c, dtype=torch.float64, device=device) for c in (xs, ys, zs))
+    ext_xy = min(X * vx, Y * vy)
+    scale = max(X * vx, Y * vy, Z * vz) / 32.0
+    rcyl = 0.45 * ext_xy
+    vol = torch.zeros((Z, Y, X), dtype=torch.float32, device=device)
+    inside = (tx[None, :] ** 2 + ty[:, None] ** 2) <= rcyl * rcyl
+    vol[:, inside] = 0.02
+    zhalf = Z * vz / 2.0
+
+    def add_blob(center, axes, rot, value):
+        r = float(np.max(axes))
+        lo = [int(np.searchsorted(c, center[k] - r)) for k, c in enumerate((xs, ys, zs))]
+        hi = [int(np.searchsorted(c, center[k] + r, side="right")) for k, c in enumerate((xs, ys, zs))]
+        if any(h <= l for l, h in zip(lo, hi)):
+            return
+        A = rot @ np.diag(1.0 / np.asarray(axes, np.float64) ** 2) @ rot.T
+        px = (tx[lo[0]:hi[0]] - center[0])[None, None, :]
+        py = (ty[lo[1]:hi[1]] - center[1])[None, :, None]
+        pz = (tz[lo[2]:hi[2]] - center[2])[:, None, None]
+        q = (A[0, 0] * px * px + A[1, 1] * py * py + A[2, 2] * pz * pz +
+             2.0 * (A[0, 1] * px * py + A[0, 2] * px * pz + A[1, 2] * py * pz))
+        vol[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] += float(np.float32(value)) * (q <= 1.0).to(torch.float32)
 
     for _ in range(n_ell):
         axes = rng.uniform(2.0, 12.0, size=3) * scale
