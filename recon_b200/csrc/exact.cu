@@ -215,7 +215,10 @@ __global__ void __launch_bounds__(256) bp_finish_kernel(ExactGeom G, const unsig
         sv[r] = (MODE == 2 && in) ? sens[i + (size_t)k0 * plane] : 0.0f;
         fv[r] = (MODE == 2 && in) ? vol[i + (size_t)k0 * plane] : 0.0f;
     }
-    const int F = fix_exponent(__ldg(maxabs), max_len, count_bits);
+    const unsigned mbits = __ldg(maxabs);
+    const int F = fix_exponent(mbits, max_len, count_bits);
+    // a non-finite input value makes every voxel NaN (as a float sum would)
+    const bool nonfinite = !isfinite(__uint_as_float(mbits));
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int x = x0 + threadIdx.y + 8 * r, y = y0 + threadIdx.x;
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(256) bp_finish_kernel(ExactGeom G, const unsig
         const size_t i = slab_off + (size_t)y * G.X + x;
         const long long q = (long long)(qa[r] + tile[threadIdx.y + 8 * r][threadIdx.x]);
         acc[i] = 0ull;
-        const float ht = (F != INT_MIN) ? (float)ldexp((double)q, -F) : 0.0f;
+        const float ht = nonfinite ? __int_as_float(0x7fffffff) : (F != INT_MIN) ? (float)ldexp((double)q, -F) : 0.0f;
         const size_t vox = i + (size_t)k0 * plane;
         if (MODE == 2) vol[vox] = (sv[r] != 0.0f) ? __fdiv_rn(__fmul_rn(fv[r], ht), sv[r]) : 0.0f;
         else vol[vox] = ht;

@@ -142,3 +142,62 @@ def test_mlem_bf16_sinogram_error_reported():
     f = P.mlem(gb, 5)
     err = rel_l2(f.cpu().numpy(), f64)
     assert err < 2e-2, err  # BF16 storage: ~3 significant digits per ratio value
+
+
+# A wide, flat volume whose back projection needs two z-slabs (768 x 768 voxels per slice:
+# 7 slices fit the 64 MiB accumulator budget), so the slab clipping, the accumulator offsets
+# and the per-slab finish are exercised against FP64.
+WIDE = small_cfg(Xdim=768, Ydim=768, Zdim=12, XVoxSize=0.05, YVoxSize=0.05, ZVoxSize=0.05, AxPixels=96,
+                 TAxPixels=24, AxPixDim=0.64, TAxPixDim=0.1, NumProj=6)
+
+
+def test_multi_slab_back_projection_vs_fp64():
+    cfg = WIDE
+    P = Plan(cfg)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    rng = np.random.default_rng(21)
+    y = rng.random(6 * g.npix).astype(np.float32)
+    bp = P.bp_views(torch.from_numpy(y).cuda().reshape(6, P.nv, P.nu)).cpu().numpy().ravel()
+    ref = O.x_bp_all(g, 6, np.float32(cfg["DeltaAng"]), y.astype(np.float64))
+    assert rel_l2(bp, ref) < 1e-5, rel_l2(bp, ref)
+    sens = P.sensitivity().cpu().numpy().ravel()
+    ref_s = O.x_bp_all(g, 6, np.float32(cfg["DeltaAng"]), np.ones(6 * g.npix))
+    assert rel_l2(sens, ref_s) < 1e-5, rel_l2(sens, ref_s)
+    x = rng.random(g.nvox).astype(np.float32)
+    fp = P.fp_views(torch.from_numpy(x).cuda().reshape(P.shape_vol)).cpu().numpy().ravel()
+    assert abs(np.dot(fp.astype(np.float64), y) - np.dot(x.astype(np.float64), bp)) < 1e-5 * abs(np.dot(fp, y))
+
+
+def test_multi_slab_mlem_vs_fp64():
+    cfg = WIDE
+    g = O.Geom.from_dict(geom_dict(cfg))
+    meas = (np.random.default_rng(22).random(6 * g.npix) * 0.05).astype(np.float32)
+    f64, _ = O.x_mlem(g, 6, np.float32(cfg["DeltaAng"]), meas, 3)
+    P = Plan(cfg)
+    f = P.mlem(torch.from_numpy(meas).cuda().reshape(6, P.nv, P.nu), 3).cpu().numpy().ravel()
+    assert rel_l2(f, f64) < 1e-4, rel_l2(f, f64)
+
+
+def test_truncated_detector_vs_fp64():
+    # a detector narrower and shorter than the volume's shadow: rays cover part of it
+    cfg = small_cfg(AxPixels=16, TAxPixels=12, NumProj=8)
+    P = Plan(cfg)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    vol = np.random.default_rng(23).random(g.nvox).astype(np.float32)
+    fp = P.fp_views(torch.from_numpy(vol).cuda().reshape(P.shape_vol)).cpu().numpy().ravel()
+    assert rel_l2(fp, _x_fp(g, cfg, vol.astype(np.float64))) < 1e-5
+    y = np.random.default_rng(24).random(8 * g.npix).astype(np.float32)
+    bp = P.bp_views(torch.from_numpy(y).cuda().reshape(8, P.nv, P.nu)).cpu().numpy().ravel()
+    assert rel_l2(bp, O.x_bp_all(g, 8, np.float32(cfg["DeltaAng"]), y.astype(np.float64))) < 1e-5
+
+
+def test_non_finite_input_gives_nan():
+    cfg = small_cfg(NumProj=4)
+    P = Plan(cfg)
+    y = torch.rand((4, P.nv, P.nu), device="cuda")
+    y[1, 3, 5] = float("nan")
+    assert torch.isnan(P.bp_views(y)).all()
+    y[1, 3, 5] = float("inf")
+    assert torch.isnan(P.bp_views(y)).all()
+    y[1, 3, 5] = 0.5  # finite again: the plan is not left in a bad state
+    assert torch.isfinite(P.bp_views(y)).all()
