@@ -118,7 +118,7 @@ __global__ void w_table_kernel(GeomD G, float* __restrict__ w)
 // with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input.
 // MODE 2: out = ratio (input of the voxel-driven back projector).
 template <bool KAHAN, int MODE, class GT, class OT>
-__global__ void __launch_bounds__(128) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
+__global__ void __launch_bounds__(128, 12) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                   const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
                                                   const float* __restrict__ wtab, const float2* __restrict__ cs,
                                                   const uint2* __restrict__ tiles, unsigned view0,

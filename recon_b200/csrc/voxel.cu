@@ -1,9 +1,11 @@
 // voxel.cu -- voxel-driven back projection (the reference's
 // backward_projection / backward_projection2, CT_Recon/hf_cuda_kernels.cuh:
-// 183-284) as a deterministic gather: one thread per voxel, a loop over views
-// inside the thread, the running sum in a register (added in view order, as
-// the reference's per-view launches add into the volume), and the MLEM update
-// f <- f * Ht / sens fused into the epilogue when requested.
+// 183-284) as a deterministic gather: a loop over views inside the thread,
+// the running sums in registers (added in view order, as the reference's
+// per-view launches add into the volume), and the MLEM update
+// f <- f * Ht / sens fused into the epilogue when requested.  One thread per
+// voxel in general; one thread per (x, y) column and z-chunk in GEOMETRIC mode
+// without detector tilt, where a column projects to one detector column.
 //
 // REFERENCE mode keeps backward_projection2's arithmetic and its flat-array
 // bilinear taps (a tap beyond the image end reads 0).  GEOMETRIC mode uses the
@@ -12,6 +14,7 @@
 // linear filtering has 8-bit weights); the reference samples through a legacy
 // texture reference with the Ruijters cubic B-spline library, which is not
 // part of the reference, so that variant cannot be reproduced.
+#include <climits>
 #include <unordered_map>
 
 #include "internal.h"
@@ -136,6 +139,93 @@ __global__ void __launch_bounds__(128) bp_kernel(VGeom G, const float* __restric
         vol[n] = (sv != 0.0f) ? __fdiv_rn(__fmul_rn(f, acc), sv) : 0.0f;
     } else {
         vol[n] = acc;
+    }
+}
+
+// GEOMETRIC mode without detector tilt (RM = I): the detector coordinates
+// of voxel (x, y, z) at a view are
+//   u = (Ry * xa / (ya + Rf) - Dx) / (du * M) + (Nu - 1) / 2,
+//   v = (Ry * z / (ya + Rf) - Dz) / (dv * M) + (Nv - 1) / 2,
+// with (xa, ya) the voxel's x-y centre rotated to the view, so u is the same
+// for a whole (x, y) column and v is linear in z.  One thread per column and
+// z-chunk of ZC voxels: per view it projects the column once, then steps v
+// along the chunk, with the ZC sums in registers.  Taps, bounds and update as
+// in bp_kernel.
+template <int ZC, int MODE, bool TEX>
+__global__ void __launch_bounds__(128) bp_column_kernel(VGeom G, const float* __restrict__ angles, unsigned view0,
+                                                         unsigned nview, unsigned Nproj,
+                                                         const float* __restrict__ sino,
+                                                         const cudaTextureObject_t* __restrict__ texs,
+                                                         float* __restrict__ vol, const float* __restrict__ sens)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = blockIdx.z * ZC;
+    if (x >= G.X || y >= G.Y) return;
+    const size_t npix = (size_t)G.Nu * G.Nv, plane = (size_t)G.X * G.Y;
+    const size_t n0 = (size_t)x + (size_t)y * G.X + (size_t)k0 * plane;
+    const int nz = min(ZC, G.Z - k0);
+    const float xo = center((float)G.X, G.vox[0], 1.0f, x);
+    const float yo = center((float)G.Y, G.vox[1], 1.0f, y);
+    const float z0 = center((float)G.Z, G.vox[2], 1.0f, k0);
+    const float inv_du = 1.0f / (G.du_mm * G.M), inv_dv = 1.0f / (G.dv_mm * G.M);
+    const float cu = (float)(G.Nu - 1) * 0.5f, cv = (float)(G.Nv - 1) * 0.5f;
+    const float umax = (float)(G.Nu - 1), vmax = (float)(G.Nv - 1);
+    const float inv_n = 1.0f / (float)Nproj;
+    float acc[ZC];
+#pragma unroll
+    for (int k = 0; k < ZC; ++k) acc[k] = (MODE == 0 && k < nz) ? vol[n0 + (size_t)k * plane] : 0.0f;
+    for (unsigned vi = 0; vi < nview; ++vi) {
+        const float alpha = angles[view0 + vi];
+        const float c = cospif(alpha / 180.0f), s = sinpif(alpha / 180.0f);
+        const float xa = xo * c - yo * s;
+        const float ya = xo * s + yo * c;
+        const float inv = 1.0f / (ya + G.Rf);
+        const float u_pix = (G.Ry * xa * inv - G.Dx) * inv_du + cu;
+        if (!(u_pix >= 0.0f && u_pix <= umax)) continue;
+        const int ui = min(max((int)floorf(u_pix), 0), G.Nu - 2);
+        const float uw = u_pix - (float)ui;
+        const float vB = G.Ry * inv * G.vox[2] * inv_dv;
+        const float vA = (G.Ry * inv * z0 - G.Dz) * inv_dv + cv;
+        const float* img = sino + vi * npix;
+        cudaTextureObject_t tex = TEX ? texs[vi] : 0;
+        // taps of rows `row` (t00, t10) and row + 1 (t01, t11), reused by the
+        // next voxel when it samples the same rows or one row further
+        int row = INT_MIN;
+        float t00 = 1.0f, t10 = 1.0f, t01 = 1.0f, t11 = 1.0f;
+#pragma unroll
+        for (int k = 0; k < ZC; ++k) {
+            const float v_pix = fmaf((float)k, vB, vA);
+            if (k < nz && v_pix >= 0.0f && v_pix <= vmax) {
+                const int vj = min(max((int)floorf(v_pix), 0), G.Nv - 2);
+                const float vw = v_pix - (float)vj;
+                if (MODE != 1 && vj != row) {
+                    if (vj == row + 1) {
+                        t00 = t01;
+                        t10 = t11;
+                    } else {
+                        t00 = tap<TEX>(img, tex, ui, vj, G.Nu);
+                        t10 = tap<TEX>(img, tex, ui + 1, vj, G.Nu);
+                    }
+                    t01 = tap<TEX>(img, tex, ui, vj + 1, G.Nu);
+                    t11 = tap<TEX>(img, tex, ui + 1, vj + 1, G.Nu);
+                    row = vj;
+                }
+                const float val = (t00 * (1.0f - uw) + t10 * uw) * (1.0f - vw) + (t01 * (1.0f - uw) + t11 * uw) * vw;
+                acc[k] = fmaf(val, inv_n, acc[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < ZC; ++k) {
+        if (k >= nz) break;
+        const size_t n = n0 + (size_t)k * plane;
+        if (MODE == 2) {
+            const float sv = sens[n];
+            vol[n] = (sv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[n], acc[k]), sv) : 0.0f;
+        } else {
+            vol[n] = acc[k];
+        }
     }
 }
 
@@ -267,12 +357,23 @@ static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angl
             d_handles = d_local;
         }
     }
-    if (tex)
+    const bool untilted = P.geom.cal.xangle == 0.0f && P.geom.cal.yangle == 0.0f && P.geom.cal.zangle == 0.0f;
+    if (VMODE == RECON_VOXEL_GEOMETRIC && untilted) {
+        constexpr int ZC = 16;
+        const dim3 cgrid((G.X + 31) / 32, (G.Y + 3) / 4, (G.Z + ZC - 1) / ZC);
+        if (tex)
+            voxel::bp_column_kernel<ZC, MODE, true><<<cgrid, blk, 0, s>>>(G, angles, first, count, Nproj, sino,
+                                                                          d_handles, vol, sens);
+        else
+            voxel::bp_column_kernel<ZC, MODE, false><<<cgrid, blk, 0, s>>>(G, angles, first, count, Nproj, sino,
+                                                                           nullptr, vol, sens);
+    } else if (tex) {
         voxel::bp_kernel<VMODE, MODE, true><<<grid, blk, 0, s>>>(G, angles, first, count, Nproj, sino, d_handles, vol,
                                                                   sens);
-    else
+    } else {
         voxel::bp_kernel<VMODE, MODE, false><<<grid, blk, 0, s>>>(G, angles, first, count, Nproj, sino, nullptr, vol,
                                                                    sens);
+    }
     cudaError_t e = cudaGetLastError();
     if (d_local) {
         // the per-call textures must outlive the kernel
