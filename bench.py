@@ -154,18 +154,35 @@ def measured_traffic() -> dict:
     return {"fp": int(m.group(1)), "bp": int(m.group(2))} if m else {}
 
 
-def batched_leg(device, n_prob: int, iters: int, opts):
+def shard_problems(work: list[float], world: int) -> list[list[int]]:
+    """Problems per rank: largest first, each to the least-loaded rank."""
+    out: list[list[int]] = [[] for _ in range(world)]
+    load = [0.0] * world
+    for p in sorted(range(len(work)), key=lambda i: -work[i]):
+        r = min(range(world), key=lambda j: load[j])
+        out[r].append(p)
+        load[r] += work[p]
+    return out
+
+
+def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int = 1):
     """48 generated problems of uneven sizes: `iters` graph-captured MLEM
     iterations of all of them through one Batch, against the same iterations
     as sequential per-problem Plan.mlem calls (sensitivities cached in both).
-    Both arms produce bit-identical images (checked here)."""
+    Both arms produce bit-identical images (checked here).  With several
+    ranks the problems are sharded by rank (no communication) and the times
+    are the max over ranks."""
     import torch
 
     from recon_b200 import Batch, Plan
     from recon_b200.configs import batched_problems
     from recon_b200.phantom import noisy, phantom
 
-    cfgs = batched_problems(n_prob, seed=4, iters=iters)
+    all_cfgs = batched_problems(n_prob, seed=4, iters=iters)
+    work = [float(c["NumProj"]) * c["AxPixels"] * c["TAxPixels"] * (c["Xdim"] + c["Ydim"] + c["Zdim"])
+            for c in all_cfgs]
+    mine = shard_problems(work, world)[rank]
+    cfgs = [all_cfgs[p] for p in mine]
     plans = [Plan(c, opts) for c in cfgs]
     gs = []
     for c, P in zip(cfgs, plans):
@@ -193,12 +210,23 @@ def batched_leg(device, n_prob: int, iters: int, opts):
     t_plain = e1.elapsed_time(e2) * 1e-3
     same = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(fb, fp))
     isects = sum(P.count_intersections() for P in plans)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([t_batch, t_plain], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_batch, t_plain = float(t[0]), float(t[1])
+        q = torch.tensor([isects, 1 if same else 0], dtype=torch.int64, device=device)
+        dist.all_reduce(q, op=dist.ReduceOp.SUM)
+        isects, same = int(q[0]), int(q[1]) == world
+    cfgs = all_cfgs
     vox = [int(c["Xdim"]) * int(c["Ydim"]) * int(c["Zdim"]) for c in cfgs]
     return {
         "problems": n_prob, "iters": iters,
         "batched_iter_s": n_prob * iters / t_batch, "plain_iter_s": n_prob * iters / t_plain,
         "speedup": t_plain / t_batch, "batched_isects_per_s": 2.0 * isects * iters / t_batch,
         "plain_isects_per_s": 2.0 * isects * iters / t_plain, "bitwise_equal": bool(same),
+        "sharding": f"problems by rank over {world} GPUs" if world > 1 else "single GPU",
         "config": {"workload": f"batched_{n_prob}_seed4", "voxels_min_max": [min(vox), max(vox)],
                    "views_min_max": [min(int(c["NumProj"]) for c in cfgs), max(int(c["NumProj"]) for c in cfgs)],
                    "isects_per_pass": isects},
@@ -428,9 +456,33 @@ def main():
     # buffers) and the read-back of step k (a third stream) overlap the
     # compute of the neighbouring steps; the timed region ends after the last
     # read-back.
-    g_host = g.cpu().pin_memory() if world == 1 else None
-    f_host = torch.empty(f.shape, dtype=torch.float32).pin_memory() if world == 1 else None
+    g_host = g.cpu().pin_memory()
+    f_host = torch.empty(f.shape, dtype=torch.float32).pin_memory()
     e2e = None
+    if world > 1:
+        # each rank uploads its own views of the sinogram, rank 0 reads the image back
+        def e2e_sharded():
+            g[first:first + count].copy_(g_host[first:first + count], non_blocking=True)
+            iteration()
+            if rank == 0:
+                f_host.copy_(f, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_sharded()
+        torch.cuda.synchronize()
+        dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            e2e_sharded()
+        b.record()
+        torch.cuda.synchronize()
+        t = torch.tensor([a.elapsed_time(b)], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item()) / args.steps
+        e2e = {"value": 1e3 / e2e_ms, "unit": UNIT,
+               "h2d_bytes_per_step": g.numel() * g.element_size(), "d2h_bytes_per_step": f.numel() * 4,
+               "pipeline": "each rank uploads its views, rank 0 reads the image back (not overlapped)"}
     if world == 1:
         comp = torch.cuda.current_stream()
         up_s, down_s = torch.cuda.Stream(), torch.cuda.Stream()
@@ -470,11 +522,6 @@ def main():
         e2e = {"value": 1e3 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": g.numel() * g.element_size(),
                "d2h_bytes_per_step": f.numel() * 4,
                "pipeline": "H2D of step k+1 and D2H of step k on their own streams, overlapping compute"}
-
-    if rank != 0:
-        if world > 1:
-            dist.destroy_process_group()
-        return
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -528,11 +575,12 @@ def main():
         del P
         torch.cuda.empty_cache()
         out["voxel_bp"] = voxel_leg(cfg, g, max(3, args.steps // 4), args.warmup, local)
-    if world == 1 and not args.no_batched:
+    if not args.no_batched:
         del g_host, f_host, g, vol
         torch.cuda.empty_cache()
-        out["batched"] = batched_leg(device, args.batched_problems, args.batched_iters, opts)
-    print(json.dumps(out))
+        out["batched"] = batched_leg(device, args.batched_problems, args.batched_iters, opts, rank, world)
+    if rank == 0:
+        print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()
 

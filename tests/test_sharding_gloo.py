@@ -114,3 +114,19 @@ def test_view_range_partition():
             ranges = [view_range(n, r, w) for r in range(w)]
             assert sum(c for _, c in ranges) == n
             assert all(ranges[r][0] + ranges[r][1] == ranges[r + 1][0] for r in range(w - 1))
+
+
+def test_batched_problems_shard_by_rank():
+    # the batched workload over several GPUs: every problem on exactly one rank,
+    # largest first to the least-loaded rank, the same split on every rank
+    import bench
+    from recon_b200.configs import batched_problems
+
+    cfgs = batched_problems(48)
+    work = [float(c["NumProj"]) * c["AxPixels"] * c["TAxPixels"] * (c["Xdim"] + c["Ydim"] + c["Zdim"]) for c in cfgs]
+    for world in (1, 2, 4, 8):
+        parts = bench.shard_problems(work, world)
+        assert sorted(p for part in parts for p in part) == list(range(48))
+        assert parts == bench.shard_problems(work, world)
+        loads = [sum(work[p] for p in part) for part in parts]
+        assert max(loads) - min(loads) <= max(work)
