@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -55,10 +56,23 @@ namespace {
 
 const int kMaxBranches = 8;
 
-std::map<std::string, int>& tune_cache()
+// Branch counts picked so far, per set of shapes (process-wide, guarded).
+std::mutex g_tune_mutex;
+std::map<std::string, int> g_tune_cache;
+
+bool tuned_branches(const std::string& key, int* k)
 {
-    static std::map<std::string, int> c;
-    return c;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it == g_tune_cache.end()) return false;
+    *k = it->second;
+    return true;
+}
+
+void remember_branches(const std::string& key, int k)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = k;
 }
 
 // one MLEM iteration of problem p on stream s
@@ -124,11 +138,7 @@ recon_status_t capture(recon_batch& b, int k)
 // images afterwards.
 recon_status_t autotune(recon_batch& b)
 {
-    auto it = tune_cache().find(b.key);
-    if (it != tune_cache().end()) {
-        b.branches = it->second;
-        return RECON_OK;
-    }
+    if (tuned_branches(b.key, &b.branches)) return RECON_OK;
     cudaStream_t origin = b.streams[0];
     size_t total = 0;
     for (auto P : b.plans) total += P->nvox;
@@ -164,7 +174,7 @@ recon_status_t autotune(recon_batch& b)
     cudaFree(save);
     RB_CUDA(cudaGetLastError());
     b.branches = pick;
-    tune_cache()[b.key] = pick;
+    remember_branches(b.key, pick);
     return RECON_OK;
 }
 

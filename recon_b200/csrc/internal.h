@@ -83,6 +83,15 @@ struct RayTiles {
     std::vector<unsigned> prefix;
 };
 
+// Texture objects over a sinogram's views, kept between voxel-driven back
+// projections of the same buffer (MLEM reuses its ratio sinogram).
+struct TexCache {
+    const float* base = nullptr;
+    unsigned count = 0;
+    cudaTextureObject_t* d_handles = nullptr;
+    std::vector<cudaTextureObject_t> handles;
+};
+
 struct Plan {
     recon_geometry_t geom{};
     recon_options_t opt{};
@@ -112,6 +121,7 @@ struct Plan {
     // back-projection z-slab; rays outside them contribute nothing
     RayTiles fp_tiles;
     std::vector<RayTiles> bp_tiles;
+    TexCache tex;  // voxel-driven back projection
     // scratch view slot for arbitrary-angle single-view calls (index nviews)
     float* d_angles = nullptr;    // [view] (float)n*DeltaAng, + 1 scratch slot
     // COMPAT tables
@@ -184,7 +194,7 @@ recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned cou
 recon_status_t plain_fp_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
 recon_status_t compat_fp_ratio_all(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
-void release_plan_textures(const Plan* P);
+void release_plan_textures(Plan* P);
 recon_status_t ensure_mlem_buffers(Plan& P);
 recon_status_t compute_sensitivity(Plan& P, float* sens, cudaStream_t s);
 recon_status_t describe_compat_geometry(const recon_geometry_t& g, Plan& P);

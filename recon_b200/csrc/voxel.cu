@@ -15,7 +15,6 @@
 // texture reference with the Ruijters cubic B-spline library, which is not
 // part of the reference, so that variant cannot be reproduced.
 #include <climits>
-#include <unordered_map>
 
 #include "internal.h"
 
@@ -297,14 +296,6 @@ static bool make_view_textures(const Plan& P, const float* sino, unsigned count,
     return true;
 }
 
-struct TexCache {
-    const float* base = nullptr;
-    unsigned count = 0;
-    cudaTextureObject_t* d_handles = nullptr;
-    std::vector<cudaTextureObject_t> handles;
-};
-static std::unordered_map<const Plan*, TexCache> g_tex_cache;
-
 static void release_textures(TexCache& c)
 {
     for (auto h : c.handles) cudaDestroyTextureObject(h);
@@ -312,14 +303,7 @@ static void release_textures(TexCache& c)
     c = TexCache{};
 }
 
-void release_plan_textures(const Plan* P)
-{
-    auto it = g_tex_cache.find(P);
-    if (it != g_tex_cache.end()) {
-        release_textures(it->second);
-        g_tex_cache.erase(it);
-    }
-}
+void release_plan_textures(Plan* P) { release_textures(P->tex); }
 
 template <int VMODE, int MODE>
 static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angles, unsigned first, unsigned count,
@@ -334,7 +318,7 @@ static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angl
     cudaTextureObject_t* d_local = nullptr;
     if (VMODE == RECON_VOXEL_GEOMETRIC && MODE != 1 && sino) {
         if (cache_textures) {
-            TexCache& c = g_tex_cache[&P];
+            TexCache& c = P.tex;
             if (c.base != sino || c.count != count) {
                 release_textures(c);
                 if (make_view_textures(P, sino, count, c.handles)) {
