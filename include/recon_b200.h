@@ -325,7 +325,10 @@ recon_status_t recon_compat_bp_view_noalloc(const recon_geometry_t* geom, const 
  * N_iteration MLEM iterations from f = 1 and writes
  * <ReconFileFolder><ReconFileNameRoot>_<it><ReconFileSuffix> after every
  * iteration plus the .info parameter echo.  `folder` may be NULL/"" (then
- * cfg is a full path).  opt may be NULL (defaults). */
+ * cfg is a full path).  opt may be NULL (defaults).  Two optional keys resume
+ * a run (no reference counterpart): InitialVolume = <raw float32 image> starts
+ * from that image instead of f = 1, StartIteration = k numbers the first
+ * iteration run k (iterations k .. N_iteration-1 run). */
 recon_status_t recon_mlem_from_cfg(const char* folder, const char* cfg,
                                    const recon_options_t* opt);
 /* siddon_recon::a1_FORWARD_PROJECTION (hf_siddon_recon.hpp:146-163,

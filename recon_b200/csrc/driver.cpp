@@ -302,6 +302,10 @@ recon_status_t write_info(const std::string& path, const recon_geometry_t& g, co
 struct Loaded {
     recon_geometry_t geom{};
     Paths paths;
+    // optional resume keys (no reference counterpart): an image to start from
+    // instead of f = 1, and the number of the first iteration to run
+    std::string initial_volume;
+    unsigned start_iteration = 0;
 };
 
 // m_check_files (hf_siddon_recon.hpp:196-226): configuration present, every
@@ -316,6 +320,8 @@ recon_status_t load_config(const char* folder, const char* cfg, Loaded& L)
     RB_TRY(load_geometry(kv, L.geom));
     RB_TRY(load_paths(kv, L.paths));
     correct_paths(L.paths);
+    if (kv.count("InitialVolume")) L.initial_volume = kv.at("InitialVolume");
+    if (kv.count("StartIteration")) RB_TRY(get_number(kv, "StartIteration", L.start_iteration));
     return RECON_OK;
 }
 
@@ -413,9 +419,15 @@ recon_status_t recon_mlem_from_cfg(const char* folder, const char* cfg, const re
     RB_TRY(d_f.alloc(nvox));
     RB_TRY(to_device(d_g.p, host.data(), host.size()));
     RB_TRY(recon_mlem_prepare(plan.p, nullptr));
-    RB_TRY(recon_set_ones(d_f.p, nvox, nullptr));
     std::vector<float> f(nvox);
-    for (unsigned it = 0; it < g.scan.N_iteration; ++it) {
+    if (L.initial_volume.empty()) {
+        RB_TRY(recon_set_ones(d_f.p, nvox, nullptr));
+    } else {
+        // resume from a saved iterate (a written <ReconFileNameRoot>_<it> file)
+        RB_TRY(read_floats(L.initial_volume, f.data(), nvox));
+        RB_TRY(to_device(d_f.p, f.data(), nvox));
+    }
+    for (unsigned it = L.start_iteration; it < g.scan.N_iteration; ++it) {
         RB_TRY(recon_mlem_iteration(plan.p, d_g.p, d_f.p, nullptr));
         RB_TRY(to_host(f.data(), d_f.p, nvox));
         RB_TRY(write_floats(numbered(L.paths.ReconFileFolder, L.paths.ReconFileNameRoot, it, L.paths.ReconFileSuffix),
