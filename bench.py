@@ -367,7 +367,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from recon_b200 import SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN, Options, Plan
+    from recon_b200 import SIDDON_BP_GATHER, SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN, Options, Plan
     from recon_b200.configs import PLAIN_GPU
     from recon_b200.sharding import ordered_sum_, view_range
 
@@ -403,12 +403,14 @@ def main():
     first, count = view_range(nviews, rank, world)
     npix = P.nu * P.nv
     nvox = f.numel()
-    # z-slabs of the back projector (librecon_b200: both int64 accumulators of a
-    # slab in 64 MiB); per step: transpose + forward, maxabs + (ray + finish) per
-    # slab, and at N > 1 a separate update
+    # kernels per step: transpose + forward; the gather back projector is one
+    # kernel, the ray-driven one maxabs + (ray + finish) per z-slab (both int64
+    # accumulators of a slab in 64 MiB); at N > 1 a separate update
+    gather = P.siddon_bp == SIDDON_BP_GATHER
     Z, Y, X = P.shape_vol
     depth = max(1, min(Z, (64 << 20) // (X * Y * 16)))
     slabs = -(-Z // depth)
+    bp_launches = 1 if gather else 1 + 2 * slabs
 
     def iteration(ev=None):
         if world == 1:
@@ -534,7 +536,8 @@ def main():
                    "l2": "no flush: per-step inputs (377 MB sinogram + 377 MB ratio) exceed the 126 MB L2"},
         "isects_per_pass": isects,
         "isects_per_s": 2.0 * isects * value,
-        "gpu_launches": args.steps * (3 + 2 * slabs if world == 1 else 4 + 2 * slabs),
+        "gpu_launches": args.steps * (2 + bp_launches + (0 if world == 1 else 1)),
+        "back_projector": "gather" if gather else "ray",
     }
     peaks = {}
     try:
@@ -550,7 +553,8 @@ def main():
         bytes_bp = 4.0 * isects + 12.0 * nvox
         traffic = measured_traffic()
         if t_bp >= t_fp:
-            dom = ("back projection (maxabs + bp_ray_kernel per z-slab + bp_finish_kernel)", t_bp, bytes_bp,
+            dom = ("back projection (bp_gather_kernel)" if gather else
+                   "back projection (maxabs + bp_ray_kernel per z-slab + bp_finish_kernel)", t_bp, bytes_bp,
                    traffic.get("bp"))
         else:
             dom = ("forward projection (transpose_xy_kernel + fp_kernel)", t_fp, bytes_fp, traffic.get("fp"))

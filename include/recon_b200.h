@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define RECON_B200_ABI_VERSION 1
+#define RECON_B200_ABI_VERSION 2
 
 typedef enum {
     RECON_OK = 0,
@@ -88,10 +88,9 @@ typedef struct {
 /* Arithmetic of the Siddon projector pair.
  *   RECON_ARITH_EXACT  -- true Siddon: every ray-voxel intersection length,
  *     plane crossings set up in FP64 and traversed in FP32, forward and back
- *     projectors exact transposes of each other (the same walk per ray), back
- *     projection summed exactly in 64-bit fixed point, so it is
- *     deterministic.  Detector tilt angles (xangle/yangle/zangle) must be
- *     zero.
+ *     projectors exact transposes of each other (the same length for every
+ *     ray-voxel pair), back projection deterministic (recon_siddon_bp_t).
+ *     Detector tilt angles (xangle/yangle/zangle) must be zero.
  *   RECON_ARITH_COMPAT -- the reference's FP32 traversal reproduced operation
  *     for operation (siddon_kernelsMLEM.cuh), including its quirks; per-ray
  *     voxel/length sequences are bit-identical to the reference's kernels on
@@ -112,6 +111,18 @@ typedef enum { RECON_BP_SIDDON = 0, RECON_BP_VOXEL = 1 } recon_bp_t;
  *   GEOMETRIC -- angle sense of the Siddon projector, coordinate converted to
  *     pixels (mm / (pitch*M)). */
 typedef enum { RECON_VOXEL_REFERENCE = 0, RECON_VOXEL_GEOMETRIC = 1 } recon_voxel_mode_t;
+/* Design of the EXACT Siddon back projector (the same lengths either way; the
+ * forward projector is unchanged).
+ *   GATHER -- one warp per (x, y) column of voxels gathers every ray that
+ *     crosses it, summing in FP32 in a fixed order (views, detector columns,
+ *     rows), so results are deterministic; no atomics.  Fastest where the rays
+ *     of adjacent detector rows cross a column at least one voxel apart.
+ *   RAY    -- one thread per ray walks it through L2-resident z-slabs and adds
+ *     into 64-bit fixed-point accumulators (exact, order-independent sums).
+ *   AUTO   -- GATHER where rows are at least a voxel apart at the depth nearest
+ *     the source and a ray's piece of one column spans less than a voxel of z;
+ *     RAY otherwise. */
+typedef enum { RECON_SIDDON_BP_AUTO = 0, RECON_SIDDON_BP_GATHER = 1, RECON_SIDDON_BP_RAY = 2 } recon_siddon_bp_t;
 
 typedef struct {
     int arith;      /* recon_arith_t, default EXACT */
@@ -120,6 +131,7 @@ typedef struct {
     int bp;         /* recon_bp_t, default SIDDON */
     int voxel_mode; /* recon_voxel_mode_t, default GEOMETRIC */
     int device;     /* CUDA device ordinal, default 0 */
+    int siddon_bp;  /* recon_siddon_bp_t, default AUTO (EXACT arithmetic only) */
 } recon_options_t;
 
 typedef struct recon_plan* recon_plan_t;
@@ -153,6 +165,10 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
 void recon_plan_destroy(recon_plan_t plan);
 /* Device bytes held by the plan. */
 size_t recon_plan_device_bytes(recon_plan_t plan);
+/* The Siddon back projector an EXACT plan uses (RECON_SIDDON_BP_GATHER or
+ * RECON_SIDDON_BP_RAY, after the AUTO choice).  No counterpart in the
+ * reference, which has one back projector. */
+recon_status_t recon_plan_siddon_bp(recon_plan_t plan, int* design);
 
 /* ---- projectors (device pointers, asynchronous on `stream`) ----------- */
 

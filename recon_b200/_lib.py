@@ -23,6 +23,7 @@ SUM_KAHAN, SUM_PLAIN = 0, 1
 SINO_F32, SINO_BF16 = 0, 1
 BP_SIDDON, BP_VOXEL = 0, 1
 VOXEL_REFERENCE, VOXEL_GEOMETRIC = 0, 1
+SIDDON_BP_AUTO, SIDDON_BP_GATHER, SIDDON_BP_RAY = 0, 1, 2
 NOALLOC_MAX_VOXELS = 2097152  # RECON_NOALLOC_MAX_VOXELS
 
 
@@ -65,7 +66,7 @@ class FilePaths(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("arith", C.c_int), ("sum", C.c_int), ("sino", C.c_int), ("bp", C.c_int),
-                ("voxel_mode", C.c_int), ("device", C.c_int)]
+                ("voxel_mode", C.c_int), ("device", C.c_int), ("siddon_bp", C.c_int)]
 
 
 _lib = None
@@ -94,6 +95,7 @@ def lib() -> C.CDLL:
         "recon_plan_create": (st, [C.POINTER(Geometry), C.POINTER(Options), C.POINTER(P)]),
         "recon_plan_destroy": (None, [P]),
         "recon_plan_device_bytes": (C.c_size_t, [P]),
+        "recon_plan_siddon_bp": (st, [P, ip]),
         "recon_fp_view": (st, [P, P, f, P, P]),
         "recon_fp_views": (st, [P, P, u, u, P, P]),
         "recon_bp_view": (st, [P, P, f, P, P]),
@@ -138,7 +140,7 @@ def exported_symbols() -> list[str]:
     """Names of the C ABI functions this binding expects (all of include/recon_b200.h)."""
     return [
         "recon_abi_version", "recon_last_error", "recon_default_options", "recon_geometry_from_cfg",
-        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_fp_view", "recon_fp_views",
+        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_fp_view", "recon_fp_views",
         "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_set_ones", "recon_divide1", "recon_multiply1",

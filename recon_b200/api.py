@@ -26,9 +26,10 @@ class Options:
     bp: int = L.BP_SIDDON
     voxel_mode: int = L.VOXEL_GEOMETRIC
     device: int = 0
+    siddon_bp: int = L.SIDDON_BP_AUTO
 
     def c(self) -> L.Options:
-        return L.Options(self.arith, self.sum, self.sino, self.bp, self.voxel_mode, self.device)
+        return L.Options(self.arith, self.sum, self.sino, self.bp, self.voxel_mode, self.device, self.siddon_bp)
 
 
 def geometry(cfg: dict) -> L.Geometry:
@@ -124,6 +125,13 @@ class Plan:
     @property
     def device_bytes(self) -> int:
         return int(lib().recon_plan_device_bytes(self._h))
+
+    @property
+    def siddon_bp(self) -> int:
+        """The Siddon back projector of an EXACT plan: SIDDON_BP_GATHER or SIDDON_BP_RAY."""
+        d = C.c_int(-1)
+        check(lib().recon_plan_siddon_bp(self._h, C.byref(d)))
+        return int(d.value)
 
     # --- tensors ---
     def new_volume(self, fill: float = 0.0):

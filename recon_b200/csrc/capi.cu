@@ -71,6 +71,9 @@ static recon_status_t validate(const recon_geometry_t& g, const recon_options_t&
     if (o.bp != RECON_BP_SIDDON && o.bp != RECON_BP_VOXEL) return fail(RECON_ERR_INVALID_ARGUMENT, "unknown bp option");
     if (o.voxel_mode != RECON_VOXEL_REFERENCE && o.voxel_mode != RECON_VOXEL_GEOMETRIC)
         return fail(RECON_ERR_INVALID_ARGUMENT, "unknown voxel_mode option");
+    if (o.siddon_bp != RECON_SIDDON_BP_AUTO && o.siddon_bp != RECON_SIDDON_BP_GATHER &&
+        o.siddon_bp != RECON_SIDDON_BP_RAY)
+        return fail(RECON_ERR_INVALID_ARGUMENT, "unknown siddon_bp option");
     if (o.arith == RECON_ARITH_EXACT) {
         if (c.xangle != 0.0f || c.yangle != 0.0f || c.zangle != 0.0f)
             return fail(RECON_ERR_UNSUPPORTED,
@@ -180,7 +183,7 @@ recon_status_t ensure_mlem_buffers(Plan& P)
     if (!P.d_ratio) {
         const size_t es = (P.opt.sino == RECON_SINO_BF16) ? 2 : 4;
         const bool per_view = (P.opt.arith == RECON_ARITH_COMPAT) && (P.opt.bp == RECON_BP_SIDDON);
-        const size_t n = per_view ? P.npix : (size_t)P.nviews * P.npix;
+        const size_t n = per_view ? P.npix : (size_t)P.nviews * mlem_ratio_view(P);
         char* q = nullptr;
         RB_CHECK(P.alloc(&q, n * es, "ratio sinogram"));
         // zero outside the ray blocks the forward projector writes (EXACT culling)
@@ -224,6 +227,7 @@ recon_status_t recon_default_options(recon_options_t* opt)
     opt->bp = RECON_BP_SIDDON;
     opt->voxel_mode = RECON_VOXEL_GEOMETRIC;
     opt->device = 0;
+    opt->siddon_bp = RECON_SIDDON_BP_AUTO;
     return RECON_OK;
 }
 
@@ -268,13 +272,21 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_cs, nv1, "view trig"));
             RB_CHECK(P->alloc(&P->d_zp, geom->det.NumTAxPixels, "ray table z"));
             RB_CHECK(P->alloc(&P->d_w, P->npix, "ray weights"));
+            P->bp_gather = opt.siddon_bp == RECON_SIDDON_BP_GATHER ||
+                           (opt.siddon_bp == RECON_SIDDON_BP_AUTO && exact_bp_gather_suits(*P));
+            RB_CHECK(P->alloc(&P->d_wq, row_quad_view(*P), "ray weights (row quads)"));
+            RB_CUDA(cudaMemset(P->d_wq, 0, row_quad_view(*P) * sizeof(float)));
+            if (P->bp_gather && P->eg.Nv > exact_bp_gather_max_rows())
+                return fail(RECON_ERR_UNSUPPORTED, "the gather back projector takes at most 14000 detector rows");
             RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
-            const size_t slab = (size_t)P->eg.X * P->eg.Y * bp_slab_depth(*P);
-            RB_CHECK(P->alloc(&P->d_bpacc, slab, "back projection accumulator"));
-            RB_CHECK(P->alloc(&P->d_bpacc_t, slab, "back projection accumulator (transposed)"));
-            RB_CHECK(P->alloc(&P->d_bpmax, 1, "back projection max"));
-            RB_CUDA(cudaMemset(P->d_bpacc, 0, slab * sizeof(unsigned long long)));
-            RB_CUDA(cudaMemset(P->d_bpacc_t, 0, slab * sizeof(unsigned long long)));
+            if (!P->bp_gather) {  // the ray-driven back projector's slab accumulators
+                const size_t slab = (size_t)P->eg.X * P->eg.Y * bp_slab_depth(*P);
+                RB_CHECK(P->alloc(&P->d_bpacc, slab, "back projection accumulator"));
+                RB_CHECK(P->alloc(&P->d_bpacc_t, slab, "back projection accumulator (transposed)"));
+                RB_CHECK(P->alloc(&P->d_bpmax, 1, "back projection max"));
+                RB_CUDA(cudaMemset(P->d_bpacc, 0, slab * sizeof(unsigned long long)));
+                RB_CUDA(cudaMemset(P->d_bpacc_t, 0, slab * sizeof(unsigned long long)));
+            }
             RB_CHECK(build_exact_tables(*P, 0));
             RB_CHECK(build_exact_culling(*P));
         } else {
@@ -298,6 +310,15 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
 void recon_plan_destroy(recon_plan_t plan) { delete plan; }
 
 size_t recon_plan_device_bytes(recon_plan_t plan) { return plan ? plan->device_bytes : 0; }
+
+recon_status_t recon_plan_siddon_bp(recon_plan_t plan, int* design)
+{
+    if (!plan || !design) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (plan->opt.arith != RECON_ARITH_EXACT)
+        return fail(RECON_ERR_UNSUPPORTED, "COMPAT plans have a single back projector");
+    *design = plan->bp_gather ? RECON_SIDDON_BP_GATHER : RECON_SIDDON_BP_RAY;
+    return RECON_OK;
+}
 
 recon_status_t recon_fp_view(recon_plan_t P, const float* d_vol, float angle, float* d_img, void* stream)
 {
@@ -433,7 +454,7 @@ recon_status_t recon_mlem_backward(recon_plan_t P, unsigned first, unsigned coun
     cudaStream_t s = as_stream(stream);
     if (count == 0) return launch_fill(d_ht, 0.0f, P->nvox, s);
     const size_t es = P->opt.sino == RECON_SINO_BF16 ? 2 : 4;
-    const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * P->npix * es;
+    const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * mlem_ratio_view(*P) * es;
     return exact_bp(*P, r, true, P->opt.sino == RECON_SINO_BF16, first, count, false, false, d_ht, nullptr, nullptr,
                     s);
 }
@@ -491,7 +512,7 @@ recon_status_t recon_osem(recon_plan_t P, const void* d_g, unsigned iters, unsig
         for (unsigned k = 0; k < n_subsets; ++k) {
             const unsigned first = k * n;
             RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, s, first, n));
-            const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * P->npix * es;
+            const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * mlem_ratio_view(*P) * es;
             RB_CHECK(exact_bp(*P, r, true, bf16, first, n, false, false, nullptr,
                               P->d_osem_sens + (size_t)k * P->nvox, d_f, s));
         }

@@ -104,26 +104,33 @@ __global__ void z_table_kernel(GeomD G, ZParam* __restrict__ zp)
     zp[v] = z;
 }
 
-__global__ void w_table_kernel(GeomD G, float* __restrict__ w)
+// w = |p2 - p1| / R per ray, stored [v][u] (w) and in the row-quad layout
+// [v/4][u][v%4] (wq)
+__global__ void w_table_kernel(GeomD G, float* __restrict__ w, float* __restrict__ wq)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int v = blockIdx.y;
     if (u >= G.Nu) return;
     const double det_x = G.R / G.Ry * (pixel_center_d(G.Nu, G.du, u) + G.Dx);
     const double det_z = G.R / G.Ry * (pixel_center_d(G.Nv, G.dv, v) + G.Dz);
-    w[(size_t)v * G.Nu + u] = (float)(sqrt(det_x * det_x + G.R * G.R + det_z * det_z) / G.R);
+    const float wv = (float)(sqrt(det_x * det_x + G.R * G.R + det_z * det_z) / G.R);
+    w[(size_t)v * G.Nu + u] = wv;
+    wq[((size_t)(v >> 2) * G.Nu + u) * 4 + (v & 3)] = wv;
 }
 
 // MODE 0: out = projection (w * sum L_t * f).  MODE 1 (MLEM): out = w * ratio
-// with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input.
-// MODE 2: out = ratio (input of the voxel-driven back projector).
+// with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input,
+// stored in the row-quad layout [view][v/4][u][v%4] when `q4` (the gather
+// back projector reads nearby rows of one detector column; a CTA's 32 x 4
+// rays fill 512 contiguous bytes) and [view][v][u] otherwise.  MODE 2: out =
+// ratio (input of the voxel-driven back projector).
 template <bool KAHAN, int MODE, class GT, class OT>
 __global__ void __launch_bounds__(128, 12) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                   const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
                                                   const float* __restrict__ wtab, const float2* __restrict__ cs,
                                                   const uint2* __restrict__ tiles, unsigned view0,
                                                   const float* __restrict__ vol, const float* __restrict__ vol_t,
-                                                  const GT* __restrict__ g, OT* __restrict__ out)
+                                                  const GT* __restrict__ g, OT* __restrict__ out, bool q4)
 {
     const RayPos R = ray_pos(tiles, view0);
     const int u = R.u, v = R.v;
@@ -144,8 +151,249 @@ __global__ void __launch_bounds__(128, 12) fp_kernel(ExactGeom G, const float4* 
     } else {
         const float gv = load_val<GT>(g + n);
         const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-        store_val<OT>(out + n, MODE == 1 ? ratio * w : ratio);
+        if (MODE == 1 && q4)
+            store_val<OT>(out + (size_t)(view - view0) * ((G.Nv + 3) >> 2) * 4 * G.Nu +
+                              ((size_t)(v >> 2) * G.Nu + u) * 4 + (v & 3),
+                          ratio * w);
+        else
+            store_val<OT>(out + n, MODE == 1 ? ratio * w : ratio);
     }
+}
+
+// ---- back projection (gather, one warp per (x, y) column) -----------------------------------
+//
+// A warp owns the column of voxels (i, j, *) and gathers, view by view, every
+// ray that crosses it; lane l owns the voxels k = k0 + l + 32 s (s < kGatherSlots)
+// of a 256-slice chunk and keeps their sums in registers.  Per view the
+// column's four corners, projected from the source, give the detector columns
+// u whose rays can cross it; for each, [A, B] is the column's piece of those
+// rays in t (from the x and y planes, evaluated as the forward walk does).  A
+// ray of row v crosses heights z = dz_v * (t + Rf) / R there, so it can meet
+// voxel [z_k, z_k+1] only if dz_v lies between min(z_k R / (A+Rf), z_k R /
+// (B+Rf)) and max(z_k+1 R / (A+Rf), z_k+1 R / (B+Rf)): a few FMAs per voxel
+// give its candidate rows (one, sometimes none or two, where rows are further
+// apart than voxels), widened by 0.01 row.  Each candidate's length
+//     L = min(B, hi_z) - max(A, lo_z)
+// takes the row's z planes exactly as the forward walk does, so the pair
+// stays an exact transpose, and is added as acc = fmaf(L, value, acc) in the
+// order views, u: each voxel's first candidate rows into a register, any
+// further ones into a shared-memory sum, and Ht = register + shared sum, so
+// the result is deterministic.
+//
+// Values are read in the row-quad layout [view][v/4][u][v%4] (view_stride
+// elements per view; 0 for the weights w of the sensitivity).  UPDATE:
+// f = (sens != 0) ? f * Ht / sens : 0; otherwise vol = Ht.
+constexpr int kGatherWarps = 8;  // a 4 x 2 tile of columns per CTA
+constexpr int kGatherSlots = 8;  // voxels per lane and chunk (chunks of 256 slices)
+
+struct GatherConst {
+    float eu, ou;  // detector column of a point (a, b) of the view frame: a / (b + Rf) * eu + ou
+    float ez, oz;  // detector row of height z at depth d (t = d - Rf):      z / d * ez + oz
+};
+
+// A warp's column seen from one view: detector columns u_lo..u_hi and, for the
+// first two, the column's piece [A, B] of their rays and the row coefficients
+// ca = ez / (A + Rf), cb = ez / (B + Rf).
+struct GatherView {
+    int u_lo, u_hi;
+    float A[2], B[2], ca[2], cb[2];
+};
+
+template <bool UPDATE, class ST>
+__global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
+    ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
+    const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned view0, unsigned nview,
+    const ST* __restrict__ vals, size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens)
+{
+    // row v's z planes: voxel k spans t in [fmaf(k - z, S, O), fmaf(k - w, S, O)]
+    // with {S, O, z, w} = szq[v] (z = kc, w = kc - 1 when S > 0; swapped when S < 0)
+    extern __shared__ float4 szq[];
+    __shared__ GatherView sview[kGatherWarps][32];
+    __shared__ float sacc2[kGatherWarps][kGatherSlots * 32];  // sums of the further candidates
+    for (int q = threadIdx.x; q < G.Nv; q += blockDim.x) {
+        const ZParam z = zp[q];
+        const float kc = (float)z.kc;
+        szq[q] = (z.S > 0.0f) ? make_float4(z.S, z.O, kc, kc - 1.0f) : make_float4(z.S, z.O, kc - 1.0f, kc);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * 4 + (warp & 3), j = blockIdx.y * 2 + (warp >> 2);
+    if (i >= G.X || j >= G.Y) return;  // whole warps; no block barrier follows
+    GatherView* sv = sview[warp];
+    float* acc2 = sacc2[warp];
+    const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
+    const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
+    const size_t plane = (size_t)G.X * G.Y;
+    const int q4row = 4 * G.Nu - 4;  // element of row v in a detector column: v + (v >> 2) * q4row
+    const float oz_lo = C.oz - 0.01f, oz_hi = C.oz + 0.01f;
+    const float dz32 = 32.0f * G.vox[2];
+    for (int k0 = 0; k0 < G.Z; k0 += 32 * kGatherSlots) {
+        const float fk0 = (float)(k0 + lane);
+        const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
+        const int nslot = min(kGatherSlots, max(0, (G.Z - k0 - lane + 31) / 32));
+        float acc[kGatherSlots];
+#pragma unroll
+        for (int s = 0; s < kGatherSlots; ++s) {
+            acc[s] = 0.0f;
+            acc2[s * 32 + lane] = 0.0f;
+        }
+        for (unsigned vb = 0; vb < nview; vb += 32) {
+            const unsigned nb = min(32u, nview - vb);
+            if ((unsigned)lane < nb) {  // lane q sets up view vb + q
+                const unsigned view = view0 + vb + lane;
+                const float2 CS = __ldg(cs + view);
+                float umin = 3.0e38f, umax = -3.0e38f;
+                bool behind = false;
+#pragma unroll
+                for (int c4 = 0; c4 < 4; ++c4) {
+                    const float X = (c4 & 1) ? Xb : Xa, Y = (c4 & 2) ? Yb : Ya;
+                    const float a = X * CS.x - Y * CS.y, b = X * CS.y + Y * CS.x;
+                    const float d = b + G.Rf;
+                    behind |= !(d > 1e-3f * G.Rf);
+                    const float uf = a / d * C.eu + C.ou;
+                    umin = fminf(umin, uf);
+                    umax = fmaxf(umax, uf);
+                }
+                GatherView V;
+                if (behind) {  // not for a volume in front of the source; stays exact anyway
+                    V.u_lo = 0;
+                    V.u_hi = G.Nu - 1;
+                } else {
+                    V.u_lo = min(max(0, __float2int_ru(umin - 0.01f)), G.Nu);
+                    V.u_hi = min(G.Nu - 1, __float2int_rd(umax + 0.01f));
+                }
+#pragma unroll
+                for (int sl = 0; sl < 2; ++sl) {
+                    const int u = min(V.u_lo + sl, G.Nu - 1);
+                    const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+                    const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+                    const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+                    const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+                    V.A[sl] = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                    V.B[sl] = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+                    V.ca[sl] = C.ez / (V.A[sl] + G.Rf);
+                    V.cb[sl] = C.ez / (V.B[sl] + G.Rf);
+                }
+                sv[lane] = V;
+            }
+            __syncwarp();
+            for (unsigned q = 0; q < nb; ++q) {
+                const unsigned vi = vb + q;
+                const int ulo = sv[q].u_lo, uhi = sv[q].u_hi;
+                for (int u = ulo; u <= uhi; ++u) {
+                    const int sl = u - ulo;
+                    float A, B, ca, cb;
+                    if (sl < 2) {
+                        A = sv[q].A[sl];
+                        B = sv[q].B[sl];
+                        ca = sv[q].ca[sl];
+                        cb = sv[q].cb[sl];
+                    } else {  // a column wider than two detector pitches: set up here
+                        const unsigned view = view0 + vi;
+                        const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+                        const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+                        const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+                        const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+                        A = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                        B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+                        ca = C.ez / (A + G.Rf);
+                        cb = C.ez / (B + G.Rf);
+                    }
+                    if (!(A < B)) continue;
+                    const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * 4;
+                    auto add = [&](int s, int v, float x) {
+                        const float4 zr = szq[v];
+                        const float t = fk0 + (float)(32 * s);
+                        const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                        const float L = fminf(B, hi) - fmaxf(A, lo);
+                        if (L > 0.0f) acc[s] = fmaf(L, x, acc[s]);
+                    };
+                    if (!(A + G.Rf > 1e-3f * G.Rf)) {  // a piece behind the source: every row is a candidate
+#pragma unroll
+                        for (int s = 0; s < kGatherSlots; ++s)
+                            if (s < nslot)
+                                for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v + (v >> 2) * q4row));
+                        continue;
+                    }
+                    // first candidate row of every voxel (loads issued together); a row that
+                    // misses the voxel gives L <= 0 and adds nothing
+                    int vl[kGatherSlots];
+                    float x[kGatherSlots];
+                    unsigned more = 0u;
+#pragma unroll
+                    for (int s = 0; s < kGatherSlots; ++s) {
+                        const float zl = fmaf((float)s, dz32, zl0), zh = fmaf((float)s, dz32, zh0);
+                        const float f0 = fminf(fmaf(zl, ca, oz_lo), fmaf(zl, cb, oz_lo));
+                        const float f1 = fmaxf(fmaf(zh, ca, oz_hi), fmaf(zh, cb, oz_hi));
+                        const int a = max(0, __float2int_ru(f0));
+                        const bool in = s < nslot && a < G.Nv;
+                        vl[s] = min(a, G.Nv - 1);
+                        x[s] = 0.0f;
+                        if (in) x[s] = load_val<ST>(col + a + (a >> 2) * q4row);
+                        if (in && (float)(a + 1) <= f1) more |= 1u << s;
+                    }
+#pragma unroll
+                    for (int s = 0; s < kGatherSlots; ++s) add(s, vl[s], x[s]);
+                    // further candidates (rare): summed apart, in shared memory
+                    if (__any_sync(0xffffffffu, more != 0u)) {
+                        for (unsigned m = more; m != 0u; m &= m - 1u) {
+                            const int s = __ffs(m) - 1;
+                            const float zl = fmaf((float)s, dz32, zl0), zh = fmaf((float)s, dz32, zh0);
+                            const int a = max(0, __float2int_ru(fminf(fmaf(zl, ca, oz_lo), fmaf(zl, cb, oz_lo))));
+                            const int b =
+                                min(G.Nv - 1, __float2int_rd(fmaxf(fmaf(zh, ca, oz_hi), fmaf(zh, cb, oz_hi))));
+                            const float t = fk0 + (float)(32 * s);
+                            float sum = acc2[s * 32 + lane];
+                            for (int v = a + 1; v <= b; ++v) {
+                                const float4 zr = szq[v];
+                                const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                                const float L = fminf(B, hi) - fmaxf(A, lo);
+                                if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v + (v >> 2) * q4row), sum);
+                            }
+                            acc2[s * 32 + lane] = sum;
+                        }
+                    }
+                }
+            }
+            __syncwarp();  // the next batch rewrites sv
+        }
+#pragma unroll
+        for (int s = 0; s < kGatherSlots; ++s) {
+            if (s >= nslot) continue;
+            const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)(k0 + lane + 32 * s) * plane;
+            const float ht = acc[s] + acc2[s * 32 + lane];
+            if (UPDATE) {
+                const float svv = sens[vox];
+                vol[vox] = (svv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[vox], ht), svv) : 0.0f;
+            } else {
+                vol[vox] = ht;
+            }
+        }
+    }
+}
+
+// A sinogram [view][v][u] (times w when WEIGHTED) in the row-quad layout
+// [view][v/4][u][v%4] that the gather reads; rows past Nv are zero.  One
+// thread per (u, row quad) of a view.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(128) to_row_quads_kernel(const float* __restrict__ in, const float* __restrict__ w,
+                                                           int Nu, int Nv, float4* __restrict__ out)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = blockIdx.y;
+    const size_t view = blockIdx.z;
+    if (u >= Nu) return;
+    float r[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int v = 4 * q + c;
+        r[c] = 0.0f;
+        if (v < Nv) {
+            r[c] = __ldg(in + (view * Nv + v) * Nu + u);
+            if (WEIGHTED) r[c] *= __ldg(w + (size_t)v * Nu + u);
+        }
+    }
+    out[(view * gridDim.y + q) * Nu + u] = make_float4(r[0], r[1], r[2], r[3]);
 }
 
 // ---- back projection (ray-driven, into a z-slab) ---------------------------------------------
@@ -293,7 +541,7 @@ recon_status_t build_exact_tables(Plan& P, cudaStream_t s)
     }
     exact::z_table_kernel<<<(G.Nv + 127) / 128, 128, 0, s>>>(G, P.d_zp);
     RB_CUDA(cudaGetLastError());
-    exact::w_table_kernel<<<dim3((G.Nu + 127) / 128, G.Nv), 128, 0, s>>>(G, P.d_w);
+    exact::w_table_kernel<<<dim3((G.Nu + 127) / 128, G.Nv), 128, 0, s>>>(G, P.d_w, P.d_wq);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
@@ -407,6 +655,7 @@ recon_status_t build_exact_culling(Plan& P)
 {
     RB_CHECK(build_ray_tiles(P, 0, P.eg.Z, P.fp_tiles));
     P.bp_tiles.clear();
+    if (P.bp_gather) return RECON_OK;  // the gather back projector needs no ray blocks
     const int depth = bp_slab_depth(P);
     for (int k0 = 0; k0 < P.eg.Z; k0 += depth) {
         P.bp_tiles.emplace_back();
@@ -453,10 +702,12 @@ static recon_status_t launch_fp(Plan& P, const float* vol, unsigned first, unsig
     const dim3 blk = fp_block();
     if (P.opt.sum == RECON_SUM_KAHAN)
         exact::fp_kernel<true, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
-                                                                  tiles, first, vol, P.d_vol_t, g, out);
+                                                                  tiles, first, vol, P.d_vol_t, g, out,
+                                                                  MODE == 1 && mlem_ratio_q4(P));
     else
         exact::fp_kernel<false, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
-                                                                   tiles, first, vol, P.d_vol_t, g, out);
+                                                                   tiles, first, vol, P.d_vol_t, g, out,
+                                                                  MODE == 1 && mlem_ratio_q4(P));
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
@@ -474,11 +725,11 @@ recon_status_t exact_fp(Plan& P, const float* vol, unsigned first, unsigned coun
 recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ratio, cudaStream_t s,
                               unsigned first, unsigned count)
 {
-    const size_t off = (size_t)first * P.npix;
+    const size_t off = (size_t)first * P.npix, roff = (size_t)first * mlem_ratio_view(P);
     using bf = __nv_bfloat16;
     if (P.opt.sino == RECON_SINO_BF16)
-        return launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + off, s);
-    return launch_fp<1, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + off, s);
+        return launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
+    return launch_fp<1, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + roff, s);
 }
 
 // Number of (ray, voxel) pairs with positive length: the forward walk with
@@ -638,6 +889,77 @@ static recon_status_t launch_bp(Plan& P, const ST* sino, unsigned first, unsigne
     return RECON_OK;
 }
 
+// The gather back projector suits geometries in which the rays of adjacent
+// detector rows cross a column at least one voxel apart in z (at the depth
+// nearest the source), so that lanes rarely meet in a voxel, and a ray's piece
+// of one column spans less than one voxel of z, so that it covers at most two.
+bool exact_bp_gather_suits(const Plan& P)
+{
+    const ExactGeom& E = P.eg;
+    const double vx = E.vox[0], vy = E.vox[1], vz = E.vox[2];
+    const double hx = 0.5 * E.X * vx, hy = 0.5 * E.Y * vy;
+    const double d_min = (double)E.Rf - std::sqrt(hx * hx + hy * hy);
+    if (!(d_min > 0.0) || !(vz > 0.0) || E.Ry == 0.0f) return false;
+    const double ry = std::fabs((double)E.Ry), dv = std::fabs((double)E.dv);
+    const double row_step = d_min * dv / (ry * vz);
+    const double slope = (0.5 * E.Nv * dv + std::fabs((double)E.Dz)) / ry;  // max |dz / d(depth)| of a ray
+    const double needle = std::sqrt(vx * vx + vy * vy) * slope / vz;
+    return row_step >= 1.0 && needle < 1.0 && E.Nv <= 3072;
+}
+
+// Largest detector row count the gather back projector takes (its rows' z
+// planes are held in shared memory, 16 bytes per row).
+int exact_bp_gather_max_rows() { return 14000; }
+
+template <bool UPDATE, class ST>
+static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride, unsigned first, unsigned count,
+                                    float* vol, const float* sens, cudaStream_t s)
+{
+    const ExactGeom& E = P.eg;
+    exact::GatherConst C;
+    C.eu = (float)((double)E.Ry / E.du);
+    C.ou = (float)(-((double)E.Dx + E.ud0) / E.du);
+    C.ez = (float)((double)E.Ry / E.dv);
+    C.oz = (float)(-((double)E.Dz + E.vd0) / E.dv);
+    const size_t smem = (size_t)E.Nv * sizeof(float4);
+    auto kernel = exact::bp_gather_kernel<UPDATE, ST>;
+    if (smem + sizeof(exact::GatherView) * 32 * exact::kGatherWarps > 48 * 1024)
+        RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 grid((E.X + 3) / 4, (E.Y + 1) / 2);
+    kernel<<<grid, exact::kGatherWarps * 32, smem, s>>>(E, C, P.d_txy, P.d_kxy, P.d_cs, P.d_zp, first, count, vals,
+                                                         view_stride, vol, sens);
+    RB_CUDA(cudaGetLastError());
+    return RECON_OK;
+}
+
+// Scratch for `count` views in the row-quad layout (grown on demand).
+static recon_status_t ensure_row_quads(Plan& P, unsigned count)
+{
+    if (P.q4_views >= count) return RECON_OK;
+    if (P.d_q4) {
+        cudaFree(P.d_q4);
+        P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), (void*)P.d_q4));
+        P.device_bytes -= (size_t)P.q4_views * row_quad_view(P) * sizeof(float);
+        P.d_q4 = nullptr;
+        P.q4_views = 0;
+    }
+    RB_CHECK(P.alloc(&P.d_q4, (size_t)count * row_quad_view(P), "row-quad sinogram"));
+    P.q4_views = count;
+    return RECON_OK;
+}
+
+// Elements per view in the row-quad layout [v/4][u][v%4].
+size_t row_quad_view(const Plan& P) { return (size_t)((P.eg.Nv + 3) / 4) * 4 * P.eg.Nu; }
+
+// The MLEM ratio is stored in the row-quad layout when the gather back
+// projector reads it, else [v][u].
+bool mlem_ratio_q4(const Plan& P)
+{
+    return P.bp_gather && P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_SIDDON;
+}
+
+size_t mlem_ratio_view(const Plan& P) { return mlem_ratio_q4(P) ? row_quad_view(P) : P.npix; }
+
 recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, unsigned first, unsigned count,
                         bool scratch_slot, bool sens_mode, float* vol, const float* sens, float* f_update,
                         cudaStream_t s)
@@ -648,12 +970,39 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
     }
     if (count == 0) return launch_fill(f_update ? f_update : vol, 0.0f, P.nvox, s);
     using bf = __nv_bfloat16;
+    if (P.bp_gather) {
+        const size_t qv = row_quad_view(P);
+        if (sens_mode) return launch_gather<false, float>(P, P.d_wq, 0, first, count, vol, nullptr, s);
+        if (sino_is_rw) {  // the MLEM ratio: row-quad layout, carries w
+            float* out = f_update ? f_update : vol;
+            if (bf16) {
+                if (f_update) return launch_gather<true, bf>(P, (const bf*)sino, qv, first, count, out, sens, s);
+                return launch_gather<false, bf>(P, (const bf*)sino, qv, first, count, out, nullptr, s);
+            }
+            if (f_update) return launch_gather<true, float>(P, (const float*)sino, qv, first, count, out, sens, s);
+            return launch_gather<false, float>(P, (const float*)sino, qv, first, count, out, nullptr, s);
+        }
+        // a sinogram [view][v][u]: weighted by w into the row-quad scratch first
+        RB_CHECK(ensure_row_quads(P, count));
+        const int nq = (P.eg.Nv + 3) / 4;
+        for (unsigned v0 = 0; v0 < count; v0 += 65535) {
+            const unsigned nv = std::min(count - v0, 65535u);
+            exact::to_row_quads_kernel<true><<<dim3((P.eg.Nu + 127) / 128, nq, nv), 128, 0, s>>>(
+                (const float*)sino + (size_t)v0 * P.npix, P.d_w, P.eg.Nu, P.eg.Nv,
+                reinterpret_cast<float4*>(P.d_q4 + (size_t)v0 * qv));
+            RB_CUDA(cudaGetLastError());
+        }
+        return launch_gather<false, float>(P, P.d_q4, qv, first, count, vol, nullptr, s);
+    }
     if (sens_mode) return launch_bp<1, false, float>(P, nullptr, first, count, vol, nullptr, s);
     if (f_update) {
         if (bf16) return launch_bp<2, false, bf>(P, (const bf*)sino, first, count, f_update, sens, s);
         return launch_bp<2, false, float>(P, (const float*)sino, first, count, f_update, sens, s);
     }
-    if (sino_is_rw) return launch_bp<0, false, float>(P, (const float*)sino, first, count, vol, nullptr, s);
+    if (sino_is_rw) {
+        if (bf16) return launch_bp<0, false, bf>(P, (const bf*)sino, first, count, vol, nullptr, s);
+        return launch_bp<0, false, float>(P, (const float*)sino, first, count, vol, nullptr, s);
+    }
     return launch_bp<0, true, float>(P, (const float*)sino, first, count, vol, nullptr, s);
 }
 

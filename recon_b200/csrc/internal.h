@@ -111,6 +111,10 @@ struct Plan {
     float2* d_cs = nullptr;    // [view] {cos, sin} of the view angle
     ZParam* d_zp = nullptr;    // [v]
     float* d_w = nullptr;      // [v][u] |p2-p1| / R
+    float* d_wq = nullptr;     // the same in the row-quad layout [v/4][u][v%4]
+    float* d_q4 = nullptr;     // a sinogram in the row-quad layout (gather back projector input)
+    unsigned q4_views = 0;     // views d_q4 holds
+    bool bp_gather = false;    // Siddon back projection by the column gather (else ray-driven slabs)
     float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y]
     // back projection: fixed-point accumulators of one z-slab, image layout
     // and xy-transposed, and the max |value| of the call's input (float bits)
@@ -202,6 +206,11 @@ recon_status_t exact_transpose(const float* vol, float* vol_t, int X, int Y, int
 int bp_count_bits(const Plan& P, unsigned nview);
 float bp_max_len(const Plan& P);
 int bp_slab_depth(const Plan& P);
+bool exact_bp_gather_suits(const Plan& P);
+int exact_bp_gather_max_rows();
+size_t mlem_ratio_view(const Plan& P);
+size_t row_quad_view(const Plan& P);
+bool mlem_ratio_q4(const Plan& P);
 recon_status_t build_exact_culling(Plan& P);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);

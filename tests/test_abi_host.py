@@ -34,14 +34,14 @@ def test_exports_every_declared_function():
     for name in declared:
         assert hasattr(lib, name), name
     assert sorted(L.exported_symbols()) == declared
-    assert lib.recon_abi_version() == 1
+    assert lib.recon_abi_version() == 2
 
 
 def test_default_options():
     o = L.Options()
     assert L.lib().recon_default_options(C.byref(o)) == 0
-    assert (o.arith, o.sum, o.sino, o.bp, o.voxel_mode, o.device) == (L.ARITH_EXACT, L.SUM_KAHAN, L.SINO_F32,
-                                                                      L.BP_SIDDON, L.VOXEL_GEOMETRIC, 0)
+    assert (o.arith, o.sum, o.sino, o.bp, o.voxel_mode, o.device, o.siddon_bp) == (
+        L.ARITH_EXACT, L.SUM_KAHAN, L.SINO_F32, L.BP_SIDDON, L.VOXEL_GEOMETRIC, 0, L.SIDDON_BP_AUTO)
 
 
 def _cfg_text(extra=""):
@@ -137,6 +137,8 @@ def test_plan_rejects_bad_geometry():
     assert lib.recon_plan_create(C.byref(geometry(small_cfg(yangle=0.01))), C.byref(o), C.byref(h)) == 2
     assert lib.recon_plan_create(C.byref(geometry(small_cfg(Rf=10.0))), C.byref(o), C.byref(h)) == 2
     o.arith = 7
+    assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1
+    o.arith, o.siddon_bp = 0, 3
     assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1
 
 

@@ -4,7 +4,10 @@ Tolerances (relative L2 against the FP64 exact Siddon of oracle/siddon_oracle.c)
   forward projection, back projection, sensitivity   <= 1e-5
   adjointness <A x, y> = <x, A^T y> (FP32 sums)        <= 1e-5
   MLEM after 10 iterations                             <= 1e-4
-Back projection and MLEM are bit-reproducible run to run.
+Back projection and MLEM are bit-reproducible run to run.  The tests that
+involve the back projector run with both of its designs (the column gather,
+FP32 sums in a fixed order, and the ray-driven walk into int64 fixed-point
+slabs), which assign the same length to every ray-voxel pair.
 """
 import numpy as np
 import pytest
@@ -18,7 +21,8 @@ if not torch.cuda.is_available():
     pytest.skip("no CUDA device", allow_module_level=True)
 
 from oracle import oracle as O  # noqa: E402
-from recon_b200 import SINO_BF16, SUM_PLAIN, Options, Plan  # noqa: E402
+from recon_b200 import (SIDDON_BP_AUTO, SIDDON_BP_GATHER, SIDDON_BP_RAY, SINO_BF16, SUM_PLAIN, Options,  # noqa: E402
+                        Plan)
 from recon_b200.configs import CPU_SMALL, geom_dict, scaled  # noqa: E402
 from recon_b200.phantom import noisy, phantom  # noqa: E402
 
@@ -29,7 +33,10 @@ GEOMS = {
     "anisotropic": small_cfg(XVoxSize=0.8, YVoxSize=1.1, ZVoxSize=0.9, Xdim=30, Ydim=26, Zdim=21, AxPixels=61,
                              TAxPixels=47),
     "cpu_small": scaled(CPU_SMALL, NumProj=18),
+    # detector rows two voxels' pitch apart: the automatic choice is the gather
+    "rows_apart": small_cfg(TAxPixDim=2.0, TAxPixels=36),
 }
+DESIGNS = {"gather": SIDDON_BP_GATHER, "ray": SIDDON_BP_RAY}
 
 
 def _x_fp(g, cfg, vol64):
@@ -51,10 +58,11 @@ def test_fp_vs_fp64(name):
     assert np.all(np.abs(ref[grazing]) < 1e-3)
 
 
+@pytest.mark.parametrize("design", list(DESIGNS))
 @pytest.mark.parametrize("name", list(GEOMS))
-def test_bp_and_sensitivity_vs_fp64(name):
+def test_bp_and_sensitivity_vs_fp64(name, design):
     cfg = GEOMS[name]
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     g = O.Geom.from_dict(geom_dict(cfg))
     nproj = int(cfg["NumProj"])
     sino = np.random.default_rng(11).random(nproj * g.npix).astype(np.float32)
@@ -66,10 +74,11 @@ def test_bp_and_sensitivity_vs_fp64(name):
     assert rel_l2(sens, sref) < 1e-5
 
 
-@pytest.mark.parametrize("name", ["plain", "offset", "cpu_small"])
-def test_adjoint(name):
+@pytest.mark.parametrize("design", list(DESIGNS))
+@pytest.mark.parametrize("name", ["plain", "offset", "cpu_small", "rows_apart"])
+def test_adjoint(name, design):
     cfg = GEOMS[name]
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     x = torch.rand(P.shape_vol, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
     y = torch.rand((P.nproj, P.nv, P.nu), device="cuda", generator=torch.Generator("cuda").manual_seed(2))
     Ax = P.fp_views(x)
@@ -79,9 +88,10 @@ def test_adjoint(name):
     assert abs(lhs - rhs) < 1e-5 * abs(lhs), (lhs, rhs)
 
 
-def test_single_view_arbitrary_angle():
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_single_view_arbitrary_angle(design):
     cfg = GEOMS["plain"]
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     g = O.Geom.from_dict(geom_dict(cfg))
     vol = np.random.default_rng(12).random(g.nvox).astype(np.float32)
     dvol = torch.from_numpy(vol).cuda().reshape(P.shape_vol)
@@ -97,9 +107,10 @@ def test_single_view_arbitrary_angle():
         assert abs(dot1 - dot2) < 1e-5 * abs(dot1)
 
 
-def test_determinism():
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_determinism(design):
     cfg = GEOMS["cpu_small"]
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     y = torch.rand((P.nproj, P.nv, P.nu), device="cuda")
     a = P.bp_views(y)
     b = P.bp_views(y)
@@ -119,25 +130,27 @@ def _mlem_case(cfg, seed):
     return g, vol, meas
 
 
+@pytest.mark.parametrize("design", list(DESIGNS))
 @pytest.mark.parametrize("opts", ["kahan", "plain_sum"])
-def test_mlem_vs_fp64(opts):
+def test_mlem_vs_fp64(opts, design):
     cfg = scaled(CPU_SMALL, Xdim=48, Ydim=48, Zdim=40, XVoxSize=0.66, YVoxSize=0.66, ZVoxSize=0.66, AxPixels=96,
                  TAxPixels=80, NumProj=45)
     g, vol, meas = _mlem_case(cfg, 3)
     iters = 10
     f64, _ = O.x_mlem(g, 45, np.float32(cfg["DeltaAng"]), meas, iters)
-    P = Plan(cfg, Options(sum=SUM_PLAIN) if opts == "plain_sum" else Options())
+    P = Plan(cfg, Options(sum=SUM_PLAIN if opts == "plain_sum" else 0, siddon_bp=DESIGNS[design]))
     f = P.mlem(torch.from_numpy(meas).cuda().reshape(45, P.nv, P.nu), iters)
     err = rel_l2(f.cpu().numpy(), f64)
     assert err < 1e-4, err
 
 
-def test_mlem_bf16_sinogram_error_reported():
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_mlem_bf16_sinogram_error_reported(design):
     cfg = scaled(CPU_SMALL, Xdim=48, Ydim=48, Zdim=40, XVoxSize=0.66, YVoxSize=0.66, ZVoxSize=0.66, AxPixels=96,
                  TAxPixels=80, NumProj=45)
     g, vol, meas = _mlem_case(cfg, 4)
     f64, _ = O.x_mlem(g, 45, np.float32(cfg["DeltaAng"]), meas, 5)
-    P = Plan(cfg, Options(sino=SINO_BF16))
+    P = Plan(cfg, Options(sino=SINO_BF16, siddon_bp=DESIGNS[design]))
     gb = torch.from_numpy(meas).cuda().reshape(45, P.nv, P.nu).to(torch.bfloat16)
     f = P.mlem(gb, 5)
     err = rel_l2(f.cpu().numpy(), f64)
@@ -151,9 +164,10 @@ WIDE = small_cfg(Xdim=768, Ydim=768, Zdim=12, XVoxSize=0.05, YVoxSize=0.05, ZVox
                  TAxPixels=24, AxPixDim=0.64, TAxPixDim=0.1, NumProj=6)
 
 
-def test_multi_slab_back_projection_vs_fp64():
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_multi_slab_back_projection_vs_fp64(design):
     cfg = WIDE
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     g = O.Geom.from_dict(geom_dict(cfg))
     rng = np.random.default_rng(21)
     y = rng.random(6 * g.npix).astype(np.float32)
@@ -168,20 +182,22 @@ def test_multi_slab_back_projection_vs_fp64():
     assert abs(np.dot(fp.astype(np.float64), y) - np.dot(x.astype(np.float64), bp)) < 1e-5 * abs(np.dot(fp, y))
 
 
-def test_multi_slab_mlem_vs_fp64():
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_multi_slab_mlem_vs_fp64(design):
     cfg = WIDE
     g = O.Geom.from_dict(geom_dict(cfg))
     meas = (np.random.default_rng(22).random(6 * g.npix) * 0.05).astype(np.float32)
     f64, _ = O.x_mlem(g, 6, np.float32(cfg["DeltaAng"]), meas, 3)
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     f = P.mlem(torch.from_numpy(meas).cuda().reshape(6, P.nv, P.nu), 3).cpu().numpy().ravel()
     assert rel_l2(f, f64) < 1e-4, rel_l2(f, f64)
 
 
-def test_truncated_detector_vs_fp64():
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_truncated_detector_vs_fp64(design):
     # a detector narrower and shorter than the volume's shadow: rays cover part of it
     cfg = small_cfg(AxPixels=16, TAxPixels=12, NumProj=8)
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     g = O.Geom.from_dict(geom_dict(cfg))
     vol = np.random.default_rng(23).random(g.nvox).astype(np.float32)
     fp = P.fp_views(torch.from_numpy(vol).cuda().reshape(P.shape_vol)).cpu().numpy().ravel()
@@ -191,13 +207,68 @@ def test_truncated_detector_vs_fp64():
     assert rel_l2(bp, O.x_bp_all(g, 8, np.float32(cfg["DeltaAng"]), y.astype(np.float64))) < 1e-5
 
 
-def test_non_finite_input_gives_nan():
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_non_finite_input(design):
+    # a non-finite value on a ray through the volume makes the voxels it crosses
+    # non-finite (the ray design's shared fixed-point scale makes every voxel NaN)
     cfg = small_cfg(NumProj=4)
-    P = Plan(cfg)
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
     y = torch.rand((4, P.nv, P.nu), device="cuda")
-    y[1, 3, 5] = float("nan")
-    assert torch.isnan(P.bp_views(y)).all()
-    y[1, 3, 5] = float("inf")
-    assert torch.isnan(P.bp_views(y)).all()
-    y[1, 3, 5] = 0.5  # finite again: the plan is not left in a bad state
+    c = (1, P.nv // 2, P.nu // 2)
+    for bad in (float("nan"), float("inf")):
+        y[c] = bad
+        out = P.bp_views(y)
+        assert not torch.isfinite(out).all()
+        if design == "ray":
+            assert torch.isnan(out).all()
+        else:
+            assert torch.isfinite(out).any()
+    y[c] = 0.5  # finite again: the plan is not left in a bad state
     assert torch.isfinite(P.bp_views(y)).all()
+
+
+def test_automatic_design_choice():
+    # rows at least a voxel apart pick the gather, rows closer than a voxel the ray walk
+    y_seed, x_seed = 31, 32
+    for name, expect in (("rows_apart", SIDDON_BP_GATHER), ("plain", SIDDON_BP_RAY)):
+        cfg = GEOMS[name]
+        auto, forced = Plan(cfg, Options(siddon_bp=SIDDON_BP_AUTO)), Plan(cfg, Options(siddon_bp=expect))
+        assert auto.siddon_bp == expect and forced.siddon_bp == expect
+        y = torch.rand((auto.nproj, auto.nv, auto.nu), device="cuda",
+                       generator=torch.Generator("cuda").manual_seed(y_seed))
+        assert torch.equal(auto.bp_views(y), forced.bp_views(y))
+        g = torch.rand((auto.nproj, auto.nv, auto.nu), device="cuda",
+                       generator=torch.Generator("cuda").manual_seed(x_seed)) * 2
+        assert torch.equal(auto.mlem(g, 2), forced.mlem(g, 2))
+
+
+@pytest.mark.parametrize("name", ["plain", "rows_apart", "anisotropic"])
+def test_designs_agree(name):
+    # both designs sum the same lengths; they differ only in FP32 summation order
+    cfg = GEOMS[name]
+    Pg, Pr = Plan(cfg, Options(siddon_bp=SIDDON_BP_GATHER)), Plan(cfg, Options(siddon_bp=SIDDON_BP_RAY))
+    y = torch.rand((Pg.nproj, Pg.nv, Pg.nu), device="cuda", generator=torch.Generator("cuda").manual_seed(33))
+    a, b = Pg.bp_views(y).double(), Pr.bp_views(y).double()
+    assert ((a - b).norm() / b.norm()).item() < 2e-6
+    a, b = Pg.sensitivity().double(), Pr.sensitivity().double()
+    assert ((a - b).norm() / b.norm()).item() < 2e-6
+
+
+# A tall, thin volume: the gather works through the column in two z-chunks (1024 + 76 voxels).
+TALL = small_cfg(Xdim=4, Ydim=4, Zdim=1100, XVoxSize=0.05, YVoxSize=0.05, ZVoxSize=0.05, AxPixels=8,
+                 TAxPixels=900, AxPixDim=0.1, TAxPixDim=0.1, NumProj=4)
+
+
+@pytest.mark.parametrize("design", list(DESIGNS))
+def test_tall_volume_vs_fp64(design):
+    cfg = TALL
+    P = Plan(cfg, Options(siddon_bp=DESIGNS[design]))
+    g = O.Geom.from_dict(geom_dict(cfg))
+    y = np.random.default_rng(25).random(4 * g.npix).astype(np.float32)
+    bp = P.bp_views(torch.from_numpy(y).cuda().reshape(4, P.nv, P.nu)).cpu().numpy().ravel()
+    ref = O.x_bp_all(g, 4, np.float32(cfg["DeltaAng"]), y.astype(np.float64))
+    assert rel_l2(bp, ref) < 1e-5, rel_l2(bp, ref)
+    meas = (np.random.default_rng(26).random(4 * g.npix) * 0.05).astype(np.float32)
+    f64, _ = O.x_mlem(g, 4, np.float32(cfg["DeltaAng"]), meas, 2)
+    f = P.mlem(torch.from_numpy(meas).cuda().reshape(4, P.nv, P.nu), 2).cpu().numpy().ravel()
+    assert rel_l2(f, f64) < 1e-4, rel_l2(f, f64)
