@@ -138,7 +138,7 @@ def make_problem(cfg, device):
     return vol, g
 
 
-TRAFFIC_PROFILE = "profiles/exact_fp_bp_plain256_360v_512.md"
+TRAFFIC_PROFILE = "profiles/exact_fp_gather_bp_plain256_360v_512.md"
 
 
 def measured_traffic() -> dict:

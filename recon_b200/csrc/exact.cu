@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 namespace rb {
 namespace exact {
@@ -120,17 +121,17 @@ __global__ void w_table_kernel(GeomD G, float* __restrict__ w, float* __restrict
 
 // MODE 0: out = projection (w * sum L_t * f).  MODE 1 (MLEM): out = w * ratio
 // with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input,
-// stored in the row-quad layout [view][v/4][u][v%4] when `q4` (the gather
-// back projector reads nearby rows of one detector column; a CTA's 32 x 4
-// rays fill 512 contiguous bytes) and [view][v][u] otherwise.  MODE 2: out =
-// ratio (input of the voxel-driven back projector).
+// stored [view][v][u].  MODE 3: the same in the row-quad layout
+// [view][v/4][u][v%4] (the gather back projector reads nearby rows of one
+// detector column; a CTA's 32 x 4 rays fill 512 contiguous bytes).  MODE 2:
+// out = ratio (input of the voxel-driven back projector).
 template <bool KAHAN, int MODE, class GT, class OT>
-__global__ void __launch_bounds__(128, 12) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
+__global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                   const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
                                                   const float* __restrict__ wtab, const float2* __restrict__ cs,
                                                   const uint2* __restrict__ tiles, unsigned view0,
                                                   const float* __restrict__ vol, const float* __restrict__ vol_t,
-                                                  const GT* __restrict__ g, OT* __restrict__ out, bool q4)
+                                                  const GT* __restrict__ g, OT* __restrict__ out)
 {
     const RayPos R = ray_pos(tiles, view0);
     const int u = R.u, v = R.v;
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(128, 12) fp_kernel(ExactGeom G, const float4* 
     } else {
         const float gv = load_val<GT>(g + n);
         const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-        if (MODE == 1 && q4)
+        if (MODE == 3)
             store_val<OT>(out + (size_t)(view - view0) * ((G.Nv + 3) >> 2) * 4 * G.Nu +
                               ((size_t)(v >> 2) * G.Nu + u) * 4 + (v & 3),
                           ratio * w);
@@ -183,7 +184,8 @@ __global__ void __launch_bounds__(128, 12) fp_kernel(ExactGeom G, const float4* 
 // Values are read in the row-quad layout [view][v/4][u][v%4] (view_stride
 // elements per view; 0 for the weights w of the sensitivity).  UPDATE:
 // f = (sens != 0) ? f * Ht / sens : 0; otherwise vol = Ht.
-constexpr int kGatherWarps = 8;  // a 4 x 2 tile of columns per CTA
+constexpr int kGatherWarps = 8;  // a kGatherTileX x (8 / kGatherTileX) tile of columns per CTA
+constexpr int kGatherTileX = 4;
 constexpr int kGatherSlots = 8;  // voxels per lane and chunk (chunks of 256 slices)
 
 struct GatherConst {
@@ -217,7 +219,8 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * 4 + (warp & 3), j = blockIdx.y * 2 + (warp >> 2);
+    const int i = blockIdx.x * kGatherTileX + warp % kGatherTileX;
+    const int j = blockIdx.y * (kGatherWarps / kGatherTileX) + warp / kGatherTileX;
     if (i >= G.X || j >= G.Y) return;  // whole warps; no block barrier follows
     GatherView* sv = sview[warp];
     float* acc2 = sacc2[warp];
@@ -237,126 +240,138 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
             acc[s] = 0.0f;
             acc2[s * 32 + lane] = 0.0f;
         }
-        for (unsigned vb = 0; vb < nview; vb += 32) {
-            const unsigned nb = min(32u, nview - vb);
-            if ((unsigned)lane < nb) {  // lane q sets up view vb + q
-                const unsigned view = view0 + vb + lane;
-                const float2 CS = __ldg(cs + view);
-                float umin = 3.0e38f, umax = -3.0e38f;
-                bool behind = false;
+        // the views' contributions to this chunk; FULL: every lane has kGatherSlots voxels
+        auto views = [&](auto full_tag) {
+            constexpr bool FULL = decltype(full_tag)::value;
+            for (unsigned vb = 0; vb < nview; vb += 32) {
+                const unsigned nb = min(32u, nview - vb);
+                if ((unsigned)lane < nb) {  // lane q sets up view vb + q
+                    const unsigned view = view0 + vb + lane;
+                    const float2 CS = __ldg(cs + view);
+                    float umin = 3.0e38f, umax = -3.0e38f;
+                    bool behind = false;
 #pragma unroll
-                for (int c4 = 0; c4 < 4; ++c4) {
-                    const float X = (c4 & 1) ? Xb : Xa, Y = (c4 & 2) ? Yb : Ya;
-                    const float a = X * CS.x - Y * CS.y, b = X * CS.y + Y * CS.x;
-                    const float d = b + G.Rf;
-                    behind |= !(d > 1e-3f * G.Rf);
-                    const float uf = a / d * C.eu + C.ou;
-                    umin = fminf(umin, uf);
-                    umax = fmaxf(umax, uf);
-                }
-                GatherView V;
-                if (behind) {  // not for a volume in front of the source; stays exact anyway
-                    V.u_lo = 0;
-                    V.u_hi = G.Nu - 1;
-                } else {
-                    V.u_lo = min(max(0, __float2int_ru(umin - 0.01f)), G.Nu);
-                    V.u_hi = min(G.Nu - 1, __float2int_rd(umax + 0.01f));
-                }
+                    for (int c4 = 0; c4 < 4; ++c4) {
+                        const float X = (c4 & 1) ? Xb : Xa, Y = (c4 & 2) ? Yb : Ya;
+                        const float a = X * CS.x - Y * CS.y, b = X * CS.y + Y * CS.x;
+                        const float d = b + G.Rf;
+                        behind |= !(d > 1e-3f * G.Rf);
+                        const float uf = a / d * C.eu + C.ou;
+                        umin = fminf(umin, uf);
+                        umax = fmaxf(umax, uf);
+                    }
+                    GatherView V;
+                    if (behind) {  // not for a volume in front of the source; stays exact anyway
+                        V.u_lo = 0;
+                        V.u_hi = G.Nu - 1;
+                    } else {
+                        V.u_lo = min(max(0, __float2int_ru(umin - 0.01f)), G.Nu);
+                        V.u_hi = min(G.Nu - 1, __float2int_rd(umax + 0.01f));
+                    }
 #pragma unroll
-                for (int sl = 0; sl < 2; ++sl) {
-                    const int u = min(V.u_lo + sl, G.Nu - 1);
-                    const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
-                    const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
-                    const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
-                    const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
-                    V.A[sl] = fmaxf(fminf(xa, xb), fminf(ya, yb));
-                    V.B[sl] = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
-                    V.ca[sl] = C.ez / (V.A[sl] + G.Rf);
-                    V.cb[sl] = C.ez / (V.B[sl] + G.Rf);
-                }
-                sv[lane] = V;
-            }
-            __syncwarp();
-            for (unsigned q = 0; q < nb; ++q) {
-                const unsigned vi = vb + q;
-                const int ulo = sv[q].u_lo, uhi = sv[q].u_hi;
-                for (int u = ulo; u <= uhi; ++u) {
-                    const int sl = u - ulo;
-                    float A, B, ca, cb;
-                    if (sl < 2) {
-                        A = sv[q].A[sl];
-                        B = sv[q].B[sl];
-                        ca = sv[q].ca[sl];
-                        cb = sv[q].cb[sl];
-                    } else {  // a column wider than two detector pitches: set up here
-                        const unsigned view = view0 + vi;
+                    for (int sl = 0; sl < 2; ++sl) {
+                        const int u = min(V.u_lo + sl, G.Nu - 1);
                         const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
                         const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
                         const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
                         const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
-                        A = fmaxf(fminf(xa, xb), fminf(ya, yb));
-                        B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
-                        ca = C.ez / (A + G.Rf);
-                        cb = C.ez / (B + G.Rf);
+                        V.A[sl] = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                        V.B[sl] = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+                        V.ca[sl] = C.ez / (V.A[sl] + G.Rf);
+                        V.cb[sl] = C.ez / (V.B[sl] + G.Rf);
                     }
-                    if (!(A < B)) continue;
-                    const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * 4;
-                    auto add = [&](int s, int v, float x) {
-                        const float4 zr = szq[v];
-                        const float t = fk0 + (float)(32 * s);
-                        const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
-                        const float L = fminf(B, hi) - fmaxf(A, lo);
-                        if (L > 0.0f) acc[s] = fmaf(L, x, acc[s]);
-                    };
-                    if (!(A + G.Rf > 1e-3f * G.Rf)) {  // a piece behind the source: every row is a candidate
-#pragma unroll
-                        for (int s = 0; s < kGatherSlots; ++s)
-                            if (s < nslot)
-                                for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v + (v >> 2) * q4row));
-                        continue;
-                    }
-                    // first candidate row of every voxel (loads issued together); a row that
-                    // misses the voxel gives L <= 0 and adds nothing
-                    int vl[kGatherSlots];
-                    float x[kGatherSlots];
-                    unsigned more = 0u;
-#pragma unroll
-                    for (int s = 0; s < kGatherSlots; ++s) {
-                        const float zl = fmaf((float)s, dz32, zl0), zh = fmaf((float)s, dz32, zh0);
-                        const float f0 = fminf(fmaf(zl, ca, oz_lo), fmaf(zl, cb, oz_lo));
-                        const float f1 = fmaxf(fmaf(zh, ca, oz_hi), fmaf(zh, cb, oz_hi));
-                        const int a = max(0, __float2int_ru(f0));
-                        const bool in = s < nslot && a < G.Nv;
-                        vl[s] = min(a, G.Nv - 1);
-                        x[s] = 0.0f;
-                        if (in) x[s] = load_val<ST>(col + a + (a >> 2) * q4row);
-                        if (in && (float)(a + 1) <= f1) more |= 1u << s;
-                    }
-#pragma unroll
-                    for (int s = 0; s < kGatherSlots; ++s) add(s, vl[s], x[s]);
-                    // further candidates (rare): summed apart, in shared memory
-                    if (__any_sync(0xffffffffu, more != 0u)) {
-                        for (unsigned m = more; m != 0u; m &= m - 1u) {
-                            const int s = __ffs(m) - 1;
-                            const float zl = fmaf((float)s, dz32, zl0), zh = fmaf((float)s, dz32, zh0);
-                            const int a = max(0, __float2int_ru(fminf(fmaf(zl, ca, oz_lo), fmaf(zl, cb, oz_lo))));
-                            const int b =
-                                min(G.Nv - 1, __float2int_rd(fmaxf(fmaf(zh, ca, oz_hi), fmaf(zh, cb, oz_hi))));
+                    sv[lane] = V;
+                }
+                __syncwarp();
+                for (unsigned q = 0; q < nb; ++q) {
+                    const unsigned vi = vb + q;
+                    const int ulo = sv[q].u_lo, uhi = sv[q].u_hi;
+                    for (int u = ulo; u <= uhi; ++u) {
+                        const int sl = u - ulo;
+                        float A, B, ca, cb;
+                        if (sl < 2) {
+                            A = sv[q].A[sl];
+                            B = sv[q].B[sl];
+                            ca = sv[q].ca[sl];
+                            cb = sv[q].cb[sl];
+                        } else {  // a column wider than two detector pitches: set up here
+                            const unsigned view = view0 + vi;
+                            const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+                            const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+                            const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+                            const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+                            A = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                            B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+                            ca = C.ez / (A + G.Rf);
+                            cb = C.ez / (B + G.Rf);
+                        }
+                        if (!(A < B)) continue;
+                        const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * 4;
+                        auto add = [&](int s, int v, float x) {
+                            const float4 zr = szq[v];
                             const float t = fk0 + (float)(32 * s);
-                            float sum = acc2[s * 32 + lane];
-                            for (int v = a + 1; v <= b; ++v) {
-                                const float4 zr = szq[v];
-                                const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
-                                const float L = fminf(B, hi) - fmaxf(A, lo);
-                                if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v + (v >> 2) * q4row), sum);
+                            const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                            const float L = fminf(B, hi) - fmaxf(A, lo);
+                            if (L > 0.0f) acc[s] = fmaf(L, x, acc[s]);
+                        };
+                        if (!(A + G.Rf > 1e-3f * G.Rf)) {  // a piece behind the source: every row is a candidate
+#pragma unroll
+                            for (int s = 0; s < kGatherSlots; ++s)
+                                if (s < nslot)
+                                    for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v + (v >> 2) * q4row));
+                            continue;
+                        }
+                        // row bounds of slot s: f0 = min over the piece of the voxel's bottom
+                        // row, f1 = max of its top row, both affine in s
+                        const float pa = dz32 * ca, pb = dz32 * cb;
+                        const float P0a = fmaf(zl0, ca, oz_lo), P0b = fmaf(zl0, cb, oz_lo);
+                        const float P1a = fmaf(zh0, ca, oz_hi), P1b = fmaf(zh0, cb, oz_hi);
+                        // first candidate row of every voxel (loads issued together); a row that
+                        // misses the voxel gives L <= 0 and adds nothing
+                        int vl[kGatherSlots];
+                        decltype(load_raw(col)) x[kGatherSlots];
+                        unsigned more = 0u;
+#pragma unroll
+                        for (int s = 0; s < kGatherSlots; ++s) {
+                            const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
+                            const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                            const int a = max(0, __float2int_ru(f0));
+                            const bool in = (FULL || s < nslot) && a < G.Nv;
+                            vl[s] = min(a, G.Nv - 1);
+                            x[s] = 0;
+                            if (in) x[s] = load_raw(col + a + (a >> 2) * q4row);
+                            if (in && (float)(a + 1) <= f1) more |= 1u << s;
+                        }
+#pragma unroll
+                        for (int s = 0; s < kGatherSlots; ++s) add(s, vl[s], widen(x[s]));
+                        // further candidates (rare): summed apart, in shared memory
+                        if (__any_sync(0xffffffffu, more != 0u)) {
+                            for (unsigned m = more; m != 0u; m &= m - 1u) {
+                                const int s = __ffs(m) - 1;
+                                const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
+                                const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                                const int a = max(0, __float2int_ru(f0));
+                                const int b = min(G.Nv - 1, __float2int_rd(f1));
+                                const float t = fk0 + (float)(32 * s);
+                                float sum = acc2[s * 32 + lane];
+                                for (int v = a + 1; v <= b; ++v) {
+                                    const float4 zr = szq[v];
+                                    const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                                    const float L = fminf(B, hi) - fmaxf(A, lo);
+                                    if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v + (v >> 2) * q4row), sum);
+                                }
+                                acc2[s * 32 + lane] = sum;
                             }
-                            acc2[s * 32 + lane] = sum;
                         }
                     }
                 }
+                __syncwarp();  // the next batch rewrites sv
             }
-            __syncwarp();  // the next batch rewrites sv
-        }
+        };
+        if (k0 + 32 * kGatherSlots <= G.Z)
+            views(std::true_type{});
+        else
+            views(std::false_type{});
 #pragma unroll
         for (int s = 0; s < kGatherSlots; ++s) {
             if (s >= nslot) continue;
@@ -686,7 +701,7 @@ static void ray_launch(const Plan& P, const RayTiles& T, unsigned first, unsigne
 // volume in the layout that suits each view (the transposed copy is made
 // here, once per call).  Only ray blocks that can cross the volume are
 // launched; the other pixels of `out` are zeroed first, except for the MLEM
-// ratio (MODE 1), whose buffer is zero outside the blocks from allocation on.
+// ratio (MODE 1 and 3), whose buffer is zero outside the blocks from allocation on.
 template <int MODE, class GT, class OT>
 static recon_status_t launch_fp(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g, OT* out,
                                 cudaStream_t s)
@@ -696,18 +711,16 @@ static recon_status_t launch_fp(Plan& P, const float* vol, unsigned first, unsig
     const uint2* tiles;
     unsigned n_launch;
     ray_launch(P, P.fp_tiles, first, count, &grid, &tiles, &n_launch);
-    if (tiles && MODE != 1) RB_CUDA(cudaMemsetAsync(out, 0, (size_t)count * P.npix * sizeof(OT), s));
+    if (tiles && MODE != 1 && MODE != 3) RB_CUDA(cudaMemsetAsync(out, 0, (size_t)count * P.npix * sizeof(OT), s));
     if (n_launch == 0) return RECON_OK;
     RB_CHECK(exact_transpose(vol, P.d_vol_t, P.eg.X, P.eg.Y, P.eg.Z, s));
     const dim3 blk = fp_block();
     if (P.opt.sum == RECON_SUM_KAHAN)
         exact::fp_kernel<true, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
-                                                                  tiles, first, vol, P.d_vol_t, g, out,
-                                                                  MODE == 1 && mlem_ratio_q4(P));
+                                                                  tiles, first, vol, P.d_vol_t, g, out);
     else
         exact::fp_kernel<false, MODE, GT, OT><<<grid, blk, 0, s>>>(P.eg, P.d_txy, P.d_kxy, P.d_zp, P.d_w, P.d_cs,
-                                                                   tiles, first, vol, P.d_vol_t, g, out,
-                                                                  MODE == 1 && mlem_ratio_q4(P));
+                                                                   tiles, first, vol, P.d_vol_t, g, out);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
@@ -727,8 +740,12 @@ recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ra
 {
     const size_t off = (size_t)first * P.npix, roff = (size_t)first * mlem_ratio_view(P);
     using bf = __nv_bfloat16;
-    if (P.opt.sino == RECON_SINO_BF16)
+    if (P.opt.sino == RECON_SINO_BF16) {
+        if (mlem_ratio_q4(P)) return launch_fp<3, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
         return launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
+    }
+    if (mlem_ratio_q4(P))
+        return launch_fp<3, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + roff, s);
     return launch_fp<1, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + roff, s);
 }
 
@@ -925,7 +942,8 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
     auto kernel = exact::bp_gather_kernel<UPDATE, ST>;
     if (smem + sizeof(exact::GatherView) * 32 * exact::kGatherWarps > 48 * 1024)
         RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const dim3 grid((E.X + 3) / 4, (E.Y + 1) / 2);
+    constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
+    const dim3 grid((E.X + tx - 1) / tx, (E.Y + ty - 1) / ty);
     kernel<<<grid, exact::kGatherWarps * 32, smem, s>>>(E, C, P.d_txy, P.d_kxy, P.d_cs, P.d_zp, first, count, vals,
                                                          view_stride, vol, sens);
     RB_CUDA(cudaGetLastError());

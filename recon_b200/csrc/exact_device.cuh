@@ -39,13 +39,26 @@ __device__ __forceinline__ int locate(float t, float S, float O, int kc, int N, 
     return i;
 }
 
-__device__ __forceinline__ float bf2f(__nv_bfloat16 x) { return __bfloat162float(x); }
 template <class T>
 __device__ __forceinline__ float load_val(const T* p);
 template <>
 __device__ __forceinline__ float load_val<float>(const float* p) { return __ldg(p); }
 template <>
-__device__ __forceinline__ float load_val<__nv_bfloat16>(const __nv_bfloat16* p) { return bf2f(*p); }
+__device__ __forceinline__ float load_val<__nv_bfloat16>(const __nv_bfloat16* p)
+{
+    // BF16 is the upper half of an FP32: widening is a shift (plain code, so a
+    // predicated load stays a predicated load)
+    return __uint_as_float((unsigned)__ldg(reinterpret_cast<const unsigned short*>(p)) << 16);
+}
+// A value as stored (load_raw) and widened to FP32 later (widen), so that a
+// batch of loads can be issued before any of them is used.
+__device__ __forceinline__ float load_raw(const float* p) { return __ldg(p); }
+__device__ __forceinline__ unsigned short load_raw(const __nv_bfloat16* p)
+{
+    return __ldg(reinterpret_cast<const unsigned short*>(p));
+}
+__device__ __forceinline__ float widen(float x) { return x; }
+__device__ __forceinline__ float widen(unsigned short h) { return __uint_as_float((unsigned)h << 16); }
 template <class T>
 __device__ __forceinline__ void store_val(T* p, float v);
 template <>
