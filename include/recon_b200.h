@@ -204,6 +204,21 @@ recon_status_t recon_sensitivity(recon_plan_t plan, float* d_sens, void* stream)
 recon_status_t recon_voxel_bp_view(recon_plan_t plan, const float* d_img, float angle_deg,
                                    unsigned int Nproj, int mode, float* d_vol_accum, void* stream);
 
+/* Ray-marching forward projection of one view at an arbitrary angle: each
+ * pixel's ray sampled on depth planes of the view's frame, every sample times
+ * the ray length per plane spacing, summed into d_img (overwritten).
+ * Replaces texture_helper3D::a1_allocate / a2_input / a3_destroy +
+ * forward_projection (hf_texture_helper.hpp:99-178, hf_cuda_kernels.cuh:
+ * 126-180), which the reference leaves without a caller.  `mode` is a
+ * recon_voxel_mode_t: REFERENCE = the kernel's arithmetic (coordinates
+ * normalised by L = (Ydim-1)*YVoxSize, point sampling with zero outside, planes
+ * at the normalised texel centres y0 = L*((k+1/2)/Ydim - 1/2), k < Ydim);
+ * GEOMETRIC = trilinear sampling at
+ * voxel centres on planes YVoxSize apart spanning the volume's bounding
+ * circle.  Any arithmetic; the view angle sense is the Siddon projector's. */
+recon_status_t recon_march_fp_view(recon_plan_t plan, const float* d_vol, float angle_deg, int mode,
+                                   float* d_img, void* stream);
+
 /* ---- MLEM --------------------------------------------------------------- */
 
 /* `iters` MLEM iterations over all NumProj views of the measured sinogram

@@ -100,6 +100,7 @@ def lib():
         L.orc_x_voxel_column.argtypes = [_GP, C.c_uint, C.c_float, C.c_int64, _i32p, _i32p, _f64p, C.c_int]
         L.orc_x_voxel_column.restype = C.c_int
         L.orc_v_bp_view.argtypes = [_GP, _f32p, C.c_float, _f32p, C.c_uint, C.c_int, _f32p]
+        L.orc_m_fp_view.argtypes = [_GP, _f32p, C.c_float, C.c_int, _f32p, _f64p]
         _lib = L
     return _lib
 
@@ -299,4 +300,12 @@ def v_bp_view(g: Geom, angle: float, img: np.ndarray, nproj: int, mode: int, vol
     out = np.zeros(g.nvox, np.float32) if vol is None else np.ascontiguousarray(vol, np.float32).copy()
     lib().orc_v_bp_view(C.byref(g), rotation_matrix(g), angle, np.ascontiguousarray(img, np.float32).ravel(),
                         nproj, mode, out)
+    return out
+
+
+def m_fp_view(g: Geom, angle: float, mode: int, vol: np.ndarray) -> np.ndarray:
+    """Ray-marching forward projection of one view (plane samples), FP64."""
+    out = np.zeros(g.npix, np.float64)
+    lib().orc_m_fp_view(C.byref(g), rotation_matrix(g), angle, mode, np.ascontiguousarray(vol, np.float32).ravel(),
+                        out)
     return out

@@ -1225,3 +1225,90 @@ void orc_v_bp_view(const orc_geom* g, const float RM[9], float angle_deg, const 
                 }
             }
 }
+
+/* ---- ray-marching forward projection ----------------------------------------
+ * forward_projection (CT_Recon/hf_cuda_kernels.cuh:126-180): a pixel's ray
+ * (pixel_iterate, :83-87, and the misalignment matrix, :140-141) is followed to
+ * depth y0 of the view's frame, rotated into the volume (:158-159) and sampled;
+ * each sample is weighted by distance_traveled (:78-81).  The reference has no
+ * caller, so the depths and the sampling follow recon_march_fp_view:
+ *   mode 0 (REFERENCE): depths at the texel centres of the normalised y
+ *     coordinate, y0 = L*((k + 1/2)/Ydim - 1/2) (k < Ydim, L =
+ *     (Ydim-1)*YVoxSize), coordinates normalised by L for every axis (:161-163),
+ *     point sampling of a normalised, border-addressed texture (texel
+ *     floor(c*size) inside [0,1), 0 outside; hf_texture_helper.hpp:113-121);
+ *   mode 1 (GEOMETRIC): depths y0 = -r + (k + 1/2)*YVoxSize spanning the
+ *     volume's bounding circle (r = half diagonal of the xy extent), trilinear
+ *     interpolation at voxel centres, 0 outside.
+ * All in FP64, except the REFERENCE angle's sine and cosine (FP32, as the GPU
+ * path computes them). */
+void orc_m_fp_view(const orc_geom* g, const float RM[9], float angle_deg, int mode, const float* vol,
+                   double* img)
+{
+    const int X = (int)g->Xdim, Y = (int)g->Ydim, Z = (int)g->Zdim;
+    const int Nu = (int)g->NumAxPixels, Nv = (int)g->NumTAxPixels;
+    const double vx = g->XVoxSize, vy = g->YVoxSize, vz = g->ZVoxSize;
+    const double P0x = -X / 2.0 * vx, P0y = -Y / 2.0 * vy, P0z = -Z / 2.0 * vz;
+    const double R = g->R, Rf = g->Rf, Ry = g->Ry, M = g->M;
+    const double du = g->AxPixDimMm, dv = g->TAxPixDimMm;
+    const double L = (Y - 1.0) * vy;
+    const size_t plane = (size_t)X * Y;
+    double c, s;
+    int nplanes;
+    double y_first;
+    if (mode == 0) {
+        const float a = angle_deg * 3.1415927f / 180.0f; /* #define M_PI, hf_cuda_kernels.cuh:23 */
+        c = (double)cosf(a);
+        s = (double)sinf(a);
+        nplanes = Y;
+        y_first = L * (0.5 / Y - 0.5);
+    } else {
+        const double pi = 3.14159265358979323846;
+        c = cos(pi * (double)angle_deg / 180.0);
+        s = sin(pi * (double)angle_deg / 180.0);
+        const double hx = 0.5 * X * vx, hy = 0.5 * Y * vy, r = sqrt(hx * hx + hy * hy);
+        nplanes = (int)ceil(2.0 * r / vy);
+        y_first = -r + 0.5 * vy;
+    }
+    for (int v = 0; v < Nv; ++v)
+        for (int u = 0; u < Nu; ++u) {
+            const double pu = -(Nu - 1.0) / 2.0 * du * M + u * du * M;
+            const double pv = -(Nv - 1.0) / 2.0 * dv * M + v * dv * M;
+            const double den = Ry + RM[3] * pu + RM[5] * pv;
+            const double u_id = R / den * (RM[0] * pu + RM[2] * pv + g->Dx);
+            const double v_id = R / den * (RM[6] * pu + RM[8] * pv + g->Dz);
+            const double w = sqrt(v_id * v_id + u_id * u_id + R * R) / R * vy;
+            double acc = 0.0;
+            const double y_step = (mode == 0) ? L / Y : vy;
+            for (int k = 0; k < nplanes; ++k) {
+                const double y0 = y_first + k * y_step;
+                const double x0 = (y0 + Rf) * u_id / R, z0 = (y0 + Rf) * v_id / R;
+                const double xa = x0 * c + y0 * s, ya = -x0 * s + y0 * c;
+                if (mode == 0) {
+                    const double xn = xa / L + 0.5, yn = ya / L + 0.5, zn = z0 / L + 0.5;
+                    if (!(xn >= 0.0 && xn < 1.0 && yn >= 0.0 && yn < 1.0 && zn >= 0.0 && zn < 1.0)) continue;
+                    int ix = (int)floor(xn * X), iy = (int)floor(yn * Y), iz = (int)floor(zn * Z);
+                    if (ix > X - 1) ix = X - 1;
+                    if (iy > Y - 1) iy = Y - 1;
+                    if (iz > Z - 1) iz = Z - 1;
+                    acc += vol[(size_t)ix + (size_t)iy * X + (size_t)iz * plane] * w;
+                } else {
+                    const double fx = (xa - P0x) / vx - 0.5, fy = (ya - P0y) / vy - 0.5, fz = (z0 - P0z) / vz - 0.5;
+                    if (!(fx > -1.0 && fx < X && fy > -1.0 && fy < Y && fz > -1.0 && fz < Z)) continue;
+                    const double gx = floor(fx), gy = floor(fy), gz = floor(fz);
+                    const int ix = (int)gx, iy = (int)gy, iz = (int)gz;
+                    const double ax = fx - gx, ay = fy - gy, az = fz - gz;
+                    double sample = 0.0;
+                    for (int t = 0; t < 8; ++t) {
+                        const int jx = ix + (t & 1), jy = iy + ((t >> 1) & 1), jz = iz + (t >> 2);
+                        if (jx < 0 || jx >= X || jy < 0 || jy >= Y || jz < 0 || jz >= Z) continue;
+                        const double wt = ((t & 1) ? ax : 1.0 - ax) * (((t >> 1) & 1) ? ay : 1.0 - ay) *
+                                          ((t >> 2) ? az : 1.0 - az);
+                        sample += wt * vol[(size_t)jx + (size_t)jy * X + (size_t)jz * plane];
+                    }
+                    acc += sample * w;
+                }
+            }
+            img[(size_t)u + (size_t)v * Nu] = acc;
+        }
+}

@@ -112,6 +112,10 @@ int orc_x_voxel_column(const orc_geom* g, unsigned int NumProj, float DeltaAng, 
 void orc_v_bp_view(const orc_geom* g, const float RM[9], float angle_deg, const float* img,
                    unsigned int Nproj, int mode, float* vol_accum);
 
+/* ---- ray-marching forward projection (plane samples, FP64) ---- */
+void orc_m_fp_view(const orc_geom* g, const float RM[9], float angle_deg, int mode, const float* vol,
+                   double* img);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,7 @@ def lib() -> C.CDLL:
         "recon_plan_destroy": (None, [P]),
         "recon_plan_device_bytes": (C.c_size_t, [P]),
         "recon_plan_siddon_bp": (st, [P, ip]),
+        "recon_march_fp_view": (st, [P, P, f, C.c_int, P, P]),
         "recon_fp_view": (st, [P, P, f, P, P]),
         "recon_fp_views": (st, [P, P, u, u, P, P]),
         "recon_bp_view": (st, [P, P, f, P, P]),
@@ -141,7 +142,7 @@ def exported_symbols() -> list[str]:
     return [
         "recon_abi_version", "recon_last_error", "recon_default_options", "recon_geometry_from_cfg",
         "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_fp_view", "recon_fp_views",
-        "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_mlem",
+        "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_march_fp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_set_ones", "recon_divide1", "recon_multiply1",
         "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_view_step_count", "recon_mlem_from_cfg",

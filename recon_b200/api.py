@@ -179,6 +179,12 @@ class Plan:
                                         _stream()))
         return accum
 
+    def march_fp_view(self, vol, angle: float, mode: int, out=None):
+        """Ray-marching forward projection of one view (plane samples; see recon_march_fp_view)."""
+        out = self.new_sinogram(1)[0] if out is None else out
+        check(lib().recon_march_fp_view(self._h, _ptr(vol), float(angle), int(mode), _ptr(out), _stream()))
+        return out
+
     # --- MLEM ---
     def mlem(self, g, iters: int, f=None, init_ones: bool = True):
         f = self.new_volume() if f is None else f

@@ -398,6 +398,19 @@ recon_status_t recon_voxel_bp_view(recon_plan_t P, const float* d_img, float ang
                     as_stream(stream));
 }
 
+recon_status_t recon_march_fp_view(recon_plan_t P, const float* d_vol, float angle, int mode, float* d_img,
+                                   void* stream)
+{
+    if (!P || !d_vol || !d_img) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (mode != RECON_VOXEL_REFERENCE && mode != RECON_VOXEL_GEOMETRIC)
+        return fail(RECON_ERR_INVALID_ARGUMENT, "unknown sampling mode");
+    if (!std::isfinite(angle)) return fail(RECON_ERR_INVALID_ARGUMENT, "angle must be finite");
+    if (mode == RECON_VOXEL_REFERENCE && P->geom.vox.Ydim < 2)
+        return fail(RECON_ERR_INVALID_ARGUMENT, "REFERENCE sampling normalises by (Ydim-1)*YVoxSize: Ydim must be at least 2");
+    RB_CHECK(use_device(*P));
+    return march_fp_view(*P, d_vol, angle, mode, d_img, as_stream(stream));
+}
+
 recon_status_t recon_mlem_prepare(recon_plan_t P, void* stream)
 {
     if (!P) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL plan");

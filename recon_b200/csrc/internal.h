@@ -207,6 +207,7 @@ int bp_count_bits(const Plan& P, unsigned nview);
 float bp_max_len(const Plan& P);
 int bp_slab_depth(const Plan& P);
 bool exact_bp_gather_suits(const Plan& P);
+recon_status_t march_fp_view(Plan& P, const float* vol, float angle_deg, int mode, float* img, cudaStream_t s);
 int exact_bp_gather_max_rows();
 size_t mlem_ratio_view(const Plan& P);
 size_t row_quad_view(const Plan& P);
