@@ -119,9 +119,10 @@ typedef enum { RECON_VOXEL_REFERENCE = 0, RECON_VOXEL_GEOMETRIC = 1 } recon_voxe
  *     of adjacent detector rows cross a column at least one voxel apart.
  *   RAY    -- one thread per ray walks it through L2-resident z-slabs and adds
  *     into 64-bit fixed-point accumulators (exact, order-independent sums).
- *   AUTO   -- GATHER where rows are at least a voxel apart at the depth nearest
- *     the source and a ray's piece of one column spans less than a voxel of z;
- *     RAY otherwise. */
+ *   AUTO   -- GATHER where the rays of adjacent rows cross a voxel column 1 to
+ *     1.4 voxels apart (at the depth nearest the source), a ray's piece of one
+ *     column spans less than a voxel of z, the volume is at least 128 voxels
+ *     tall and the detector has at most 3072 rows; RAY otherwise. */
 typedef enum { RECON_SIDDON_BP_AUTO = 0, RECON_SIDDON_BP_GATHER = 1, RECON_SIDDON_BP_RAY = 2 } recon_siddon_bp_t;
 
 typedef struct {

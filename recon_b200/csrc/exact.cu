@@ -164,8 +164,8 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
 // ---- back projection (gather, one warp per (x, y) column) -----------------------------------
 //
 // A warp owns the column of voxels (i, j, *) and gathers, view by view, every
-// ray that crosses it; lane l owns the voxels k = k0 + l + 32 s (s < kGatherSlots)
-// of a 256-slice chunk and keeps their sums in registers.  Per view the
+// ray that crosses it; lane l owns the voxels k = k0 + l + 32 s (s < SLOTS) of
+// a chunk of 32 * SLOTS slices and keeps their sums in registers.  Per view the
 // column's four corners, projected from the source, give the detector columns
 // u whose rays can cross it; for each, [A, B] is the column's piece of those
 // rays in t (from the x and y planes, evaluated as the forward walk does).  A
@@ -186,7 +186,8 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
 // f = (sens != 0) ? f * Ht / sens : 0; otherwise vol = Ht.
 constexpr int kGatherWarps = 8;  // a kGatherTileX x (8 / kGatherTileX) tile of columns per CTA
 constexpr int kGatherTileX = 4;
-constexpr int kGatherSlots = 8;  // voxels per lane and chunk (chunks of 256 slices)
+// SLOTS: voxels per lane and chunk (chunks of 32 * SLOTS slices; 8 unless the
+// volume is shorter)
 
 struct GatherConst {
     float eu, ou;  // detector column of a point (a, b) of the view frame: a / (b + Rf) * eu + ou
@@ -201,7 +202,7 @@ struct GatherView {
     float A[2], B[2], ca[2], cb[2];
 };
 
-template <bool UPDATE, class ST>
+template <bool UPDATE, class ST, int SLOTS>
 __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
     const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned view0, unsigned nview,
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     // with {S, O, z, w} = szq[v] (z = kc, w = kc - 1 when S > 0; swapped when S < 0)
     extern __shared__ float4 szq[];
     __shared__ GatherView sview[kGatherWarps][32];
-    __shared__ float sacc2[kGatherWarps][kGatherSlots * 32];  // sums of the further candidates
+    __shared__ float sacc2[kGatherWarps][SLOTS * 32];  // sums of the further candidates
     for (int q = threadIdx.x; q < G.Nv; q += blockDim.x) {
         const ZParam z = zp[q];
         const float kc = (float)z.kc;
@@ -230,17 +231,17 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     const int q4row = 4 * G.Nu - 4;  // element of row v in a detector column: v + (v >> 2) * q4row
     const float oz_lo = C.oz - 0.01f, oz_hi = C.oz + 0.01f;
     const float dz32 = 32.0f * G.vox[2];
-    for (int k0 = 0; k0 < G.Z; k0 += 32 * kGatherSlots) {
+    for (int k0 = 0; k0 < G.Z; k0 += 32 * SLOTS) {
         const float fk0 = (float)(k0 + lane);
         const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
-        const int nslot = min(kGatherSlots, max(0, (G.Z - k0 - lane + 31) / 32));
-        float acc[kGatherSlots];
+        const int nslot = min(SLOTS, max(0, (G.Z - k0 - lane + 31) / 32));
+        float acc[SLOTS];
 #pragma unroll
-        for (int s = 0; s < kGatherSlots; ++s) {
+        for (int s = 0; s < SLOTS; ++s) {
             acc[s] = 0.0f;
             acc2[s * 32 + lane] = 0.0f;
         }
-        // the views' contributions to this chunk; FULL: every lane has kGatherSlots voxels
+        // the views' contributions to this chunk; FULL: every lane has SLOTS voxels
         auto views = [&](auto full_tag) {
             constexpr bool FULL = decltype(full_tag)::value;
             for (unsigned vb = 0; vb < nview; vb += 32) {
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                         };
                         if (!(A + G.Rf > 1e-3f * G.Rf)) {  // a piece behind the source: every row is a candidate
 #pragma unroll
-                            for (int s = 0; s < kGatherSlots; ++s)
+                            for (int s = 0; s < SLOTS; ++s)
                                 if (s < nslot)
                                     for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v + (v >> 2) * q4row));
                             continue;
@@ -328,11 +329,11 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                         const float P1a = fmaf(zh0, ca, oz_hi), P1b = fmaf(zh0, cb, oz_hi);
                         // first candidate row of every voxel (loads issued together); a row that
                         // misses the voxel gives L <= 0 and adds nothing
-                        int vl[kGatherSlots];
-                        decltype(load_raw(col)) x[kGatherSlots];
+                        int vl[SLOTS];
+                        decltype(load_raw(col)) x[SLOTS];
                         unsigned more = 0u;
 #pragma unroll
-                        for (int s = 0; s < kGatherSlots; ++s) {
+                        for (int s = 0; s < SLOTS; ++s) {
                             const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
                             const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
                             const int a = max(0, __float2int_ru(f0));
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                             if (in && (float)(a + 1) <= f1) more |= 1u << s;
                         }
 #pragma unroll
-                        for (int s = 0; s < kGatherSlots; ++s) add(s, vl[s], widen(x[s]));
+                        for (int s = 0; s < SLOTS; ++s) add(s, vl[s], widen(x[s]));
                         // further candidates (rare): summed apart, in shared memory
                         if (__any_sync(0xffffffffu, more != 0u)) {
                             for (unsigned m = more; m != 0u; m &= m - 1u) {
@@ -368,12 +369,12 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                 __syncwarp();  // the next batch rewrites sv
             }
         };
-        if (k0 + 32 * kGatherSlots <= G.Z)
+        if (k0 + 32 * SLOTS <= G.Z)
             views(std::true_type{});
         else
             views(std::false_type{});
 #pragma unroll
-        for (int s = 0; s < kGatherSlots; ++s) {
+        for (int s = 0; s < SLOTS; ++s) {
             if (s >= nslot) continue;
             const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)(k0 + lane + 32 * s) * plane;
             const float ht = acc[s] + acc2[s * 32 + lane];
@@ -906,10 +907,16 @@ static recon_status_t launch_bp(Plan& P, const ST* sino, unsigned first, unsigne
     return RECON_OK;
 }
 
-// The gather back projector suits geometries in which the rays of adjacent
-// detector rows cross a column at least one voxel apart in z (at the depth
-// nearest the source), so that lanes rarely meet in a voxel, and a ray's piece
-// of one column spans less than one voxel of z, so that it covers at most two.
+// The gather back projector is the faster one where each voxel has about one
+// candidate row per detector column and view: the rays of adjacent detector
+// rows cross a column 1 to 1.4 voxels apart in z (at the depth nearest the
+// source; closer rows give voxels several candidates, further ones leave many
+// voxels without one while the gather still pays for them), a ray's piece of
+// one column spans less than one voxel of z, and columns are at least 128
+// voxels tall (shorter ones leave the per-view set-up unamortised).  Measured
+// on one B200: 0.75x the ray design's time at 256^3 / 360 views / 512^2,
+// 0.93x at 128^3; 0.90-0.97x on the generated problems inside these bounds and
+// 1.1-2.2x outside them.
 bool exact_bp_gather_suits(const Plan& P)
 {
     const ExactGeom& E = P.eg;
@@ -921,16 +928,16 @@ bool exact_bp_gather_suits(const Plan& P)
     const double row_step = d_min * dv / (ry * vz);
     const double slope = (0.5 * E.Nv * dv + std::fabs((double)E.Dz)) / ry;  // max |dz / d(depth)| of a ray
     const double needle = std::sqrt(vx * vx + vy * vy) * slope / vz;
-    return row_step >= 1.0 && needle < 1.0 && E.Nv <= 3072;
+    return row_step >= 1.0 && row_step <= 1.4 && needle < 1.0 && E.Nv <= 3072 && E.Z >= 128;
 }
 
 // Largest detector row count the gather back projector takes (its rows' z
 // planes are held in shared memory, 16 bytes per row).
 int exact_bp_gather_max_rows() { return 14000; }
 
-template <bool UPDATE, class ST>
-static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride, unsigned first, unsigned count,
-                                    float* vol, const float* sens, cudaStream_t s)
+template <bool UPDATE, class ST, int SLOTS>
+static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_stride, unsigned first,
+                                          unsigned count, float* vol, const float* sens, cudaStream_t s)
 {
     const ExactGeom& E = P.eg;
     exact::GatherConst C;
@@ -939,7 +946,7 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
     C.ez = (float)((double)E.Ry / E.dv);
     C.oz = (float)(-((double)E.Dz + E.vd0) / E.dv);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
-    auto kernel = exact::bp_gather_kernel<UPDATE, ST>;
+    auto kernel = exact::bp_gather_kernel<UPDATE, ST, SLOTS>;
     if (smem + sizeof(exact::GatherView) * 32 * exact::kGatherWarps > 48 * 1024)
         RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
@@ -948,6 +955,34 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
                                                          view_stride, vol, sens);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
+}
+
+// Voxels per lane: the volume's height in as few chunks of at most 8 x 32
+// slices as possible, split evenly (a lane's slots beyond the volume cost
+// as much as used ones).
+int gather_slots(int Z)
+{
+    const int chunks = (Z + 255) / 256;
+    return std::min(8, std::max(1, (Z + 32 * chunks - 1) / (32 * chunks)));
+}
+
+template <bool UPDATE, class ST>
+static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride, unsigned first, unsigned count,
+                                    float* vol, const float* sens, cudaStream_t s)
+{
+#define RB_GATHER_SLOTS(n) \
+    case n: return launch_gather_slots<UPDATE, ST, n>(P, vals, view_stride, first, count, vol, sens, s)
+    switch (gather_slots(P.eg.Z)) {
+        RB_GATHER_SLOTS(1);
+        RB_GATHER_SLOTS(2);
+        RB_GATHER_SLOTS(3);
+        RB_GATHER_SLOTS(4);
+        RB_GATHER_SLOTS(5);
+        RB_GATHER_SLOTS(6);
+        RB_GATHER_SLOTS(7);
+        default: return launch_gather_slots<UPDATE, ST, 8>(P, vals, view_stride, first, count, vol, sens, s);
+    }
+#undef RB_GATHER_SLOTS
 }
 
 // Scratch for `count` views in the row-quad layout (grown on demand).

@@ -33,8 +33,12 @@ GEOMS = {
     "anisotropic": small_cfg(XVoxSize=0.8, YVoxSize=1.1, ZVoxSize=0.9, Xdim=30, Ydim=26, Zdim=21, AxPixels=61,
                              TAxPixels=47),
     "cpu_small": scaled(CPU_SMALL, NumProj=18),
-    # detector rows two voxels' pitch apart: the automatic choice is the gather
+    # detector rows 1.2 voxels apart (a short volume, so the automatic choice stays the ray walk)
     "rows_apart": small_cfg(TAxPixDim=2.0, TAxPixels=36),
+    # 100 and 256 slices: the gather's 4- and 8-voxel-per-lane variants (the others
+    # cover 1, 2 and, in TALL below, 7)
+    "z100": small_cfg(Zdim=100, TAxPixels=110, NumProj=8),
+    "z256": small_cfg(Xdim=16, Ydim=16, Zdim=256, ZVoxSize=0.25, TAxPixDim=0.5, TAxPixels=160, NumProj=6),
 }
 DESIGNS = {"gather": SIDDON_BP_GATHER, "ray": SIDDON_BP_RAY}
 
@@ -228,9 +232,10 @@ def test_non_finite_input(design):
 
 
 def test_automatic_design_choice():
-    # rows at least a voxel apart pick the gather, rows closer than a voxel the ray walk
+    # rows 1 to 1.4 voxels apart on a tall volume pick the gather; rows closer than a
+    # voxel, or a short volume, the ray walk
     y_seed, x_seed = 31, 32
-    for name, expect in (("rows_apart", SIDDON_BP_GATHER), ("plain", SIDDON_BP_RAY)):
+    for name, expect in (("z256", SIDDON_BP_GATHER), ("plain", SIDDON_BP_RAY), ("rows_apart", SIDDON_BP_RAY)):
         cfg = GEOMS[name]
         auto, forced = Plan(cfg, Options(siddon_bp=SIDDON_BP_AUTO)), Plan(cfg, Options(siddon_bp=expect))
         assert auto.siddon_bp == expect and forced.siddon_bp == expect
@@ -254,7 +259,7 @@ def test_designs_agree(name):
     assert ((a - b).norm() / b.norm()).item() < 2e-6
 
 
-# A tall, thin volume: the gather works through the column in two z-chunks (1024 + 76 voxels).
+# A tall, thin volume: the gather works through the column in five z-chunks of 224 slices.
 TALL = small_cfg(Xdim=4, Ydim=4, Zdim=1100, XVoxSize=0.05, YVoxSize=0.05, ZVoxSize=0.05, AxPixels=8,
                  TAxPixels=900, AxPixDim=0.1, TAxPixDim=0.1, NumProj=4)
 
