@@ -388,10 +388,9 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     }
 }
 
-// A sinogram [view][v][u] (times w when WEIGHTED) in the row-quad layout
-// [view][v/4][u][v%4] that the gather reads; rows past Nv are zero.  One
-// thread per (u, row quad) of a view.
-template <bool WEIGHTED>
+// A sinogram [view][v][u] times w in the row-quad layout [view][v/4][u][v%4]
+// that the gather reads; rows past Nv are zero.  One thread per (u, row quad)
+// of a view.
 __global__ void __launch_bounds__(128) to_row_quads_kernel(const float* __restrict__ in, const float* __restrict__ w,
                                                            int Nu, int Nv, float4* __restrict__ out)
 {
@@ -405,8 +404,7 @@ __global__ void __launch_bounds__(128) to_row_quads_kernel(const float* __restri
         const int v = 4 * q + c;
         r[c] = 0.0f;
         if (v < Nv) {
-            r[c] = __ldg(in + (view * Nv + v) * Nu + u);
-            if (WEIGHTED) r[c] *= __ldg(w + (size_t)v * Nu + u);
+            r[c] = __ldg(in + (view * Nv + v) * Nu + u) * __ldg(w + (size_t)v * Nu + u);
         }
     }
     out[(view * gridDim.y + q) * Nu + u] = make_float4(r[0], r[1], r[2], r[3]);
@@ -1040,7 +1038,7 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
         const int nq = (P.eg.Nv + 3) / 4;
         for (unsigned v0 = 0; v0 < count; v0 += 65535) {
             const unsigned nv = std::min(count - v0, 65535u);
-            exact::to_row_quads_kernel<true><<<dim3((P.eg.Nu + 127) / 128, nq, nv), 128, 0, s>>>(
+            exact::to_row_quads_kernel<<<dim3((P.eg.Nu + 127) / 128, nq, nv), 128, 0, s>>>(
                 (const float*)sino + (size_t)v0 * P.npix, P.d_w, P.eg.Nu, P.eg.Nv,
                 reinterpret_cast<float4*>(P.d_q4 + (size_t)v0 * qv));
             RB_CUDA(cudaGetLastError());
