@@ -277,7 +277,7 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_wq, row_quad_view(*P), "ray weights (row quads)"));
             RB_CUDA(cudaMemset(P->d_wq, 0, row_quad_view(*P) * sizeof(float)));
             if (P->bp_gather && P->eg.Nv > exact_bp_gather_max_rows())
-                return fail(RECON_ERR_UNSUPPORTED, "the gather back projector takes at most 14000 detector rows");
+                return fail(RECON_ERR_UNSUPPORTED, "the gather back projector takes at most 12288 detector rows");
             RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
             if (!P->bp_gather) {  // the ray-driven back projector's slab accumulators
                 const size_t slab = (size_t)P->eg.X * P->eg.Y * bp_slab_depth(*P);

@@ -929,9 +929,10 @@ bool exact_bp_gather_suits(const Plan& P)
     return row_step >= 1.0 && row_step <= 1.4 && needle < 1.0 && E.Nv <= 3072 && E.Z >= 128;
 }
 
-// Largest detector row count the gather back projector takes (its rows' z
-// planes are held in shared memory, 16 bytes per row).
-int exact_bp_gather_max_rows() { return 14000; }
+// Largest detector row count the gather back projector takes: its rows' z
+// planes are held in shared memory, 16 bytes per row, beside 18 KB of per-warp
+// arrays, within the 227 KB a block may use.
+int exact_bp_gather_max_rows() { return 12288; }
 
 template <bool UPDATE, class ST, int SLOTS>
 static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_stride, unsigned first,
@@ -945,7 +946,9 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
     C.oz = (float)(-((double)E.Dz + E.vd0) / E.dv);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
     auto kernel = exact::bp_gather_kernel<UPDATE, ST, SLOTS>;
-    if (smem + sizeof(exact::GatherView) * 32 * exact::kGatherWarps > 48 * 1024)
+    const size_t static_smem = sizeof(exact::GatherView) * 32 * exact::kGatherWarps +  // sview
+                               sizeof(float) * exact::kGatherWarps * SLOTS * 32;         // sacc2
+    if (smem + static_smem > 48 * 1024)
         RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
     const dim3 grid((E.X + tx - 1) / tx, (E.Y + ty - 1) / ty);

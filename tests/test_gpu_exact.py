@@ -277,3 +277,17 @@ def test_tall_volume_vs_fp64(design):
     f64, _ = O.x_mlem(g, 4, np.float32(cfg["DeltaAng"]), meas, 2)
     f = P.mlem(torch.from_numpy(meas).cuda().reshape(4, P.nv, P.nu), 2).cpu().numpy().ravel()
     assert rel_l2(f, f64) < 1e-4, rel_l2(f, f64)
+
+
+def test_gather_with_many_detector_rows():
+    # 4000 rows: the rows' z-plane table (64 KB) needs the large shared-memory opt-in;
+    # the gather must agree with the ray walk.  Past 12288 rows a forced gather is refused.
+    cfg = small_cfg(Xdim=8, Ydim=8, Zdim=200, ZVoxSize=0.2, AxPixels=16, TAxPixels=4000, TAxPixDim=0.05,
+                    NumProj=3)
+    Pg, Pr = Plan(cfg, Options(siddon_bp=SIDDON_BP_GATHER)), Plan(cfg, Options(siddon_bp=SIDDON_BP_RAY))
+    y = torch.rand((3, Pg.nv, Pg.nu), device="cuda", generator=torch.Generator("cuda").manual_seed(35))
+    a, b = Pg.bp_views(y).double(), Pr.bp_views(y).double()
+    assert b.norm() > 0 and ((a - b).norm() / b.norm()).item() < 2e-6
+    with pytest.raises(Exception):
+        Plan(small_cfg(AxPixels=2, TAxPixels=12289), Options(siddon_bp=SIDDON_BP_GATHER))
+    assert Plan(small_cfg(AxPixels=2, TAxPixels=12289)).siddon_bp == SIDDON_BP_RAY
