@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
 // voxel [z_k, z_k+1] only if dz_v lies between min(z_k R / (A+Rf), z_k R /
 // (B+Rf)) and max(z_k+1 R / (A+Rf), z_k+1 R / (B+Rf)): a few FMAs per voxel
 // give its candidate rows (one, sometimes none or two, where rows are further
-// apart than voxels), widened by 0.01 row.  Each candidate's length
+// apart than voxels), widened by 0.002 row.  Each candidate's length
 //     L = min(B, hi_z) - max(A, lo_z)
 // takes the row's z planes exactly as the forward walk does, so the pair
 // stays an exact transpose, and is added as acc = fmaf(L, value, acc) in the
@@ -229,7 +229,10 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
     const size_t plane = (size_t)G.X * G.Y;
     const int q4row = 4 * G.Nu - 4;  // element of row v in a detector column: v + (v >> 2) * q4row
-    const float oz_lo = C.oz - 0.01f, oz_hi = C.oz + 0.01f;
+    // candidate rows are widened by 0.002 row on either side: about ten times the
+    // FP32 error of the row bounds (values of a few hundred rows, a few roundings),
+    // small enough that a voxel rarely shows a second candidate that is not one
+    const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;
     const float dz32 = 32.0f * G.vox[2];
     for (int k0 = 0; k0 < G.Z; k0 += 32 * SLOTS) {
         const float fk0 = (float)(k0 + lane);
@@ -327,24 +330,42 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                         const float pa = dz32 * ca, pb = dz32 * cb;
                         const float P0a = fmaf(zl0, ca, oz_lo), P0b = fmaf(zl0, cb, oz_lo);
                         const float P1a = fmaf(zh0, ca, oz_hi), P1b = fmaf(zh0, cb, oz_hi);
+                        // The candidate interval's length f1 - f0 is convex in s (a max of
+                        // affine functions minus a min of them), so its largest value over
+                        // the slots is at s = 0 or s = SLOTS - 1: when both are under one
+                        // row, no voxel of the lane has a second candidate.
+                        const float s_last = (float)(SLOTS - 1);
+                        const float len = fmaxf(fmaxf(P1a, P1b) - fminf(P0a, P0b),
+                                                fmaxf(fmaf(s_last, pa, P1a), fmaf(s_last, pb, P1b)) -
+                                                    fminf(fmaf(s_last, pa, P0a), fmaf(s_last, pb, P0b)));
+                        const bool single = __all_sync(0xffffffffu, len < 0.999f);
                         // first candidate row of every voxel (loads issued together); a row that
                         // misses the voxel gives L <= 0 and adds nothing
-                        int vl[SLOTS];
-                        decltype(load_raw(col)) x[SLOTS];
                         unsigned more = 0u;
+                        auto first_rows = [&](auto single_tag) {
+                            constexpr bool SINGLE = decltype(single_tag)::value;
+                            int vl[SLOTS];
+                            decltype(load_raw(col)) x[SLOTS];
 #pragma unroll
-                        for (int s = 0; s < SLOTS; ++s) {
-                            const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
-                            const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
-                            const int a = max(0, __float2int_ru(f0));
-                            const bool in = (FULL || s < nslot) && a < G.Nv;
-                            vl[s] = min(a, G.Nv - 1);
-                            x[s] = 0;
-                            if (in) x[s] = load_raw(col + a + (a >> 2) * q4row);
-                            if (in && (float)(a + 1) <= f1) more |= 1u << s;
-                        }
+                            for (int s = 0; s < SLOTS; ++s) {
+                                const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
+                                const int a = max(0, __float2int_ru(f0));
+                                const bool in = (FULL || s < nslot) && a < G.Nv;
+                                vl[s] = min(a, G.Nv - 1);
+                                x[s] = 0;
+                                if (in) x[s] = load_raw(col + a + (a >> 2) * q4row);
+                                if (!SINGLE) {
+                                    const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                                    if (in && (float)(a + 1) <= f1) more |= 1u << s;
+                                }
+                            }
 #pragma unroll
-                        for (int s = 0; s < SLOTS; ++s) add(s, vl[s], widen(x[s]));
+                            for (int s = 0; s < SLOTS; ++s) add(s, vl[s], widen(x[s]));
+                        };
+                        if (single)
+                            first_rows(std::true_type{});
+                        else
+                            first_rows(std::false_type{});
                         // further candidates (rare): summed apart, in shared memory
                         if (__any_sync(0xffffffffu, more != 0u)) {
                             for (unsigned m = more; m != 0u; m &= m - 1u) {
