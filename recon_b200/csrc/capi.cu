@@ -274,8 +274,8 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_w, P->npix, "ray weights"));
             P->bp_gather = opt.siddon_bp == RECON_SIDDON_BP_GATHER ||
                            (opt.siddon_bp == RECON_SIDDON_BP_AUTO && exact_bp_gather_suits(*P));
-            RB_CHECK(P->alloc(&P->d_wq, row_quad_view(*P), "ray weights (row quads)"));
-            RB_CUDA(cudaMemset(P->d_wq, 0, row_quad_view(*P) * sizeof(float)));
+            RB_CHECK(P->alloc(&P->d_wq, row_group_view(*P), "ray weights (row groups)"));
+            RB_CUDA(cudaMemset(P->d_wq, 0, row_group_view(*P) * sizeof(float)));
             if (P->bp_gather && P->eg.Nv > exact_bp_gather_max_rows())
                 return fail(RECON_ERR_UNSUPPORTED, "the gather back projector takes at most 12288 detector rows");
             RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));

@@ -105,7 +105,7 @@ __global__ void z_table_kernel(GeomD G, ZParam* __restrict__ zp)
     zp[v] = z;
 }
 
-// w = |p2 - p1| / R per ray, stored [v][u] (w) and in the row-quad layout
+// w = |p2 - p1| / R per ray, stored [v][u] (w) and in the row-group layout
 // [v/4][u][v%4] (wq)
 __global__ void w_table_kernel(GeomD G, float* __restrict__ w, float* __restrict__ wq)
 {
@@ -116,14 +116,15 @@ __global__ void w_table_kernel(GeomD G, float* __restrict__ w, float* __restrict
     const double det_z = G.R / G.Ry * (pixel_center_d(G.Nv, G.dv, v) + G.Dz);
     const float wv = (float)(sqrt(det_x * det_x + G.R * G.R + det_z * det_z) / G.R);
     w[(size_t)v * G.Nu + u] = wv;
-    wq[((size_t)(v >> 2) * G.Nu + u) * 4 + (v & 3)] = wv;
+    wq[((size_t)(v >> kRowGroupShift) * G.Nu + u) * kRowGroup + (v & (kRowGroup - 1))] = wv;
 }
 
 // MODE 0: out = projection (w * sum L_t * f).  MODE 1 (MLEM): out = w * ratio
 // with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input,
-// stored [view][v][u].  MODE 3: the same in the row-quad layout
-// [view][v/4][u][v%4] (the gather back projector reads nearby rows of one
-// detector column; a CTA's 32 x 4 rays fill 512 contiguous bytes).  MODE 2:
+// stored [view][v][u].  MODE 3: the same in the row-group layout
+// [view][v/8][u][v%8] (the gather back projector reads nearby rows of one
+// detector column; a CTA's 32 x 4 rays fill the halves of 32 row groups, which
+// the neighbouring row block completes).  MODE 2:
 // out = ratio (input of the voxel-driven back projector).
 template <bool KAHAN, int MODE, class GT, class OT>
 __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
@@ -153,8 +154,8 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
         const float gv = load_val<GT>(g + n);
         const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
         if (MODE == 3)
-            store_val<OT>(out + (size_t)(view - view0) * ((G.Nv + 3) >> 2) * 4 * G.Nu +
-                              ((size_t)(v >> 2) * G.Nu + u) * 4 + (v & 3),
+            store_val<OT>(out + (size_t)(view - view0) * ((G.Nv + kRowGroup - 1) >> kRowGroupShift) * kRowGroup * G.Nu +
+                              ((size_t)(v >> kRowGroupShift) * G.Nu + u) * kRowGroup + (v & (kRowGroup - 1)),
                           ratio * w);
         else
             store_val<OT>(out + n, MODE == 1 ? ratio * w : ratio);
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
 // further ones into a shared-memory sum, and Ht = register + shared sum, so
 // the result is deterministic.
 //
-// Values are read in the row-quad layout [view][v/4][u][v%4] (view_stride
+// Values are read in the row-group layout [view][v/8][u][v%8] (view_stride
 // elements per view; 0 for the weights w of the sensitivity).  UPDATE:
 // f = (sens != 0) ? f * Ht / sens : 0; otherwise vol = Ht.
 constexpr int kGatherWarps = 8;  // a kGatherTileX x (8 / kGatherTileX) tile of columns per CTA
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
     const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
     const size_t plane = (size_t)G.X * G.Y;
-    const int q4row = 4 * G.Nu - 4;  // element of row v in a detector column: v + (v >> 2) * q4row
+    const int grow = kRowGroup * G.Nu - kRowGroup;  // element of row v in a detector column: v + (v / kRowGroup) * grow
     // candidate rows are widened by 0.002 row on either side: about ten times the
     // FP32 error of the row bounds (values of a few hundred rows, a few roundings),
     // small enough that a voxel rarely shows a second candidate that is not one
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                             cb = C.ez / (B + G.Rf);
                         }
                         if (!(A < B)) continue;
-                        const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * 4;
+                        const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * kRowGroup;
                         auto add = [&](int s, int v, float x) {
                             const float4 zr = szq[v];
                             const float t = fk0 + (float)(32 * s);
@@ -322,7 +323,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
 #pragma unroll
                             for (int s = 0; s < SLOTS; ++s)
                                 if (s < nslot)
-                                    for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v + (v >> 2) * q4row));
+                                    for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v + (v >> kRowGroupShift) * grow));
                             continue;
                         }
                         // row bounds of slot s: f0 = min over the piece of the voxel's bottom
@@ -353,7 +354,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                                 const bool in = (FULL || s < nslot) && a < G.Nv;
                                 vl[s] = min(a, G.Nv - 1);
                                 x[s] = 0;
-                                if (in) x[s] = load_raw(col + a + (a >> 2) * q4row);
+                                if (in) x[s] = load_raw(col + a + (a >> kRowGroupShift) * grow);
                                 if (!SINGLE) {
                                     const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
                                     if (in && (float)(a + 1) <= f1) more |= 1u << s;
@@ -380,7 +381,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                                     const float4 zr = szq[v];
                                     const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
                                     const float L = fminf(B, hi) - fmaxf(A, lo);
-                                    if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v + (v >> 2) * q4row), sum);
+                                    if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v + (v >> kRowGroupShift) * grow), sum);
                                 }
                                 acc2[s * 32 + lane] = sum;
                             }
@@ -409,26 +410,26 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     }
 }
 
-// A sinogram [view][v][u] times w in the row-quad layout [view][v/4][u][v%4]
-// that the gather reads; rows past Nv are zero.  One thread per (u, row quad)
+// A sinogram [view][v][u] times w in the row-group layout [view][v/8][u][v%8]
+// that the gather reads; rows past Nv are zero.  One thread per (u, row group)
 // of a view.
-__global__ void __launch_bounds__(128) to_row_quads_kernel(const float* __restrict__ in, const float* __restrict__ w,
+__global__ void __launch_bounds__(128) to_row_groups_kernel(const float* __restrict__ in, const float* __restrict__ w,
                                                            int Nu, int Nv, float4* __restrict__ out)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int q = blockIdx.y;
     const size_t view = blockIdx.z;
     if (u >= Nu) return;
-    float r[4];
+    float r[kRowGroup];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int v = 4 * q + c;
+    for (int c = 0; c < kRowGroup; ++c) {
+        const int v = kRowGroup * q + c;
         r[c] = 0.0f;
-        if (v < Nv) {
-            r[c] = __ldg(in + (view * Nv + v) * Nu + u) * __ldg(w + (size_t)v * Nu + u);
-        }
+        if (v < Nv) r[c] = __ldg(in + (view * Nv + v) * Nu + u) * __ldg(w + (size_t)v * Nu + u);
     }
-    out[(view * gridDim.y + q) * Nu + u] = make_float4(r[0], r[1], r[2], r[3]);
+    float4* o = out + ((view * gridDim.y + q) * Nu + u) * (kRowGroup / 4);
+#pragma unroll
+    for (int c = 0; c < kRowGroup / 4; ++c) o[c] = make_float4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
 }
 
 // ---- back projection (ray-driven, into a z-slab) ---------------------------------------------
@@ -761,10 +762,10 @@ recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ra
     const size_t off = (size_t)first * P.npix, roff = (size_t)first * mlem_ratio_view(P);
     using bf = __nv_bfloat16;
     if (P.opt.sino == RECON_SINO_BF16) {
-        if (mlem_ratio_q4(P)) return launch_fp<3, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
+        if (mlem_ratio_grouped(P)) return launch_fp<3, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
         return launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
     }
-    if (mlem_ratio_q4(P))
+    if (mlem_ratio_grouped(P))
         return launch_fp<3, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + roff, s);
     return launch_fp<1, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + roff, s);
 }
@@ -1007,33 +1008,33 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
 #undef RB_GATHER_SLOTS
 }
 
-// Scratch for `count` views in the row-quad layout (grown on demand).
-static recon_status_t ensure_row_quads(Plan& P, unsigned count)
+// Scratch for `count` views in the row-group layout (grown on demand).
+static recon_status_t ensure_row_groups(Plan& P, unsigned count)
 {
-    if (P.q4_views >= count) return RECON_OK;
-    if (P.d_q4) {
-        cudaFree(P.d_q4);
-        P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), (void*)P.d_q4));
-        P.device_bytes -= (size_t)P.q4_views * row_quad_view(P) * sizeof(float);
-        P.d_q4 = nullptr;
-        P.q4_views = 0;
+    if (P.rowgroup_views >= count) return RECON_OK;
+    if (P.d_rowgroups) {
+        cudaFree(P.d_rowgroups);
+        P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), (void*)P.d_rowgroups));
+        P.device_bytes -= (size_t)P.rowgroup_views * row_group_view(P) * sizeof(float);
+        P.d_rowgroups = nullptr;
+        P.rowgroup_views = 0;
     }
-    RB_CHECK(P.alloc(&P.d_q4, (size_t)count * row_quad_view(P), "row-quad sinogram"));
-    P.q4_views = count;
+    RB_CHECK(P.alloc(&P.d_rowgroups, (size_t)count * row_group_view(P), "row-group sinogram"));
+    P.rowgroup_views = count;
     return RECON_OK;
 }
 
-// Elements per view in the row-quad layout [v/4][u][v%4].
-size_t row_quad_view(const Plan& P) { return (size_t)((P.eg.Nv + 3) / 4) * 4 * P.eg.Nu; }
+// Elements per view in the row-group layout [v/8][u][v%8].
+size_t row_group_view(const Plan& P) { return (size_t)((P.eg.Nv + kRowGroup - 1) / kRowGroup) * kRowGroup * P.eg.Nu; }
 
-// The MLEM ratio is stored in the row-quad layout when the gather back
+// The MLEM ratio is stored in the row-group layout when the gather back
 // projector reads it, else [v][u].
-bool mlem_ratio_q4(const Plan& P)
+bool mlem_ratio_grouped(const Plan& P)
 {
     return P.bp_gather && P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_SIDDON;
 }
 
-size_t mlem_ratio_view(const Plan& P) { return mlem_ratio_q4(P) ? row_quad_view(P) : P.npix; }
+size_t mlem_ratio_view(const Plan& P) { return mlem_ratio_grouped(P) ? row_group_view(P) : P.npix; }
 
 recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, unsigned first, unsigned count,
                         bool scratch_slot, bool sens_mode, float* vol, const float* sens, float* f_update,
@@ -1046,9 +1047,9 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
     if (count == 0) return launch_fill(f_update ? f_update : vol, 0.0f, P.nvox, s);
     using bf = __nv_bfloat16;
     if (P.bp_gather) {
-        const size_t qv = row_quad_view(P);
+        const size_t qv = row_group_view(P);
         if (sens_mode) return launch_gather<false, float>(P, P.d_wq, 0, first, count, vol, nullptr, s);
-        if (sino_is_rw) {  // the MLEM ratio: row-quad layout, carries w
+        if (sino_is_rw) {  // the MLEM ratio: row-group layout, carries w
             float* out = f_update ? f_update : vol;
             if (bf16) {
                 if (f_update) return launch_gather<true, bf>(P, (const bf*)sino, qv, first, count, out, sens, s);
@@ -1057,17 +1058,17 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
             if (f_update) return launch_gather<true, float>(P, (const float*)sino, qv, first, count, out, sens, s);
             return launch_gather<false, float>(P, (const float*)sino, qv, first, count, out, nullptr, s);
         }
-        // a sinogram [view][v][u]: weighted by w into the row-quad scratch first
-        RB_CHECK(ensure_row_quads(P, count));
-        const int nq = (P.eg.Nv + 3) / 4;
+        // a sinogram [view][v][u]: weighted by w into the row-group scratch first
+        RB_CHECK(ensure_row_groups(P, count));
+        const int nq = (P.eg.Nv + kRowGroup - 1) / kRowGroup;
         for (unsigned v0 = 0; v0 < count; v0 += 65535) {
             const unsigned nv = std::min(count - v0, 65535u);
-            exact::to_row_quads_kernel<<<dim3((P.eg.Nu + 127) / 128, nq, nv), 128, 0, s>>>(
+            exact::to_row_groups_kernel<<<dim3((P.eg.Nu + 127) / 128, nq, nv), 128, 0, s>>>(
                 (const float*)sino + (size_t)v0 * P.npix, P.d_w, P.eg.Nu, P.eg.Nv,
-                reinterpret_cast<float4*>(P.d_q4 + (size_t)v0 * qv));
+                reinterpret_cast<float4*>(P.d_rowgroups + (size_t)v0 * qv));
             RB_CUDA(cudaGetLastError());
         }
-        return launch_gather<false, float>(P, P.d_q4, qv, first, count, vol, nullptr, s);
+        return launch_gather<false, float>(P, P.d_rowgroups, qv, first, count, vol, nullptr, s);
     }
     if (sens_mode) return launch_bp<1, false, float>(P, nullptr, first, count, vol, nullptr, s);
     if (f_update) {

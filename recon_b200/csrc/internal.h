@@ -111,9 +111,9 @@ struct Plan {
     float2* d_cs = nullptr;    // [view] {cos, sin} of the view angle
     ZParam* d_zp = nullptr;    // [v]
     float* d_w = nullptr;      // [v][u] |p2-p1| / R
-    float* d_wq = nullptr;     // the same in the row-quad layout [v/4][u][v%4]
-    float* d_q4 = nullptr;     // a sinogram in the row-quad layout (gather back projector input)
-    unsigned q4_views = 0;     // views d_q4 holds
+    float* d_wq = nullptr;     // the same in the row-group layout [v/8][u][v%8]
+    float* d_rowgroups = nullptr;  // a sinogram in the row-group layout (gather back projector input)
+    unsigned rowgroup_views = 0;   // views d_rowgroups holds
     bool bp_gather = false;    // Siddon back projection by the column gather (else ray-driven slabs)
     float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y]
     // back projection: fixed-point accumulators of one z-slab, image layout
@@ -210,8 +210,11 @@ bool exact_bp_gather_suits(const Plan& P);
 recon_status_t march_fp_view(Plan& P, const float* vol, float angle_deg, int mode, float* img, cudaStream_t s);
 int exact_bp_gather_max_rows();
 size_t mlem_ratio_view(const Plan& P);
-size_t row_quad_view(const Plan& P);
-bool mlem_ratio_q4(const Plan& P);
+// Row-group layout of sinograms read by the gather back projector:
+// [view][v / kRowGroup][u][v % kRowGroup].
+constexpr int kRowGroup = 8, kRowGroupShift = 3;
+size_t row_group_view(const Plan& P);
+bool mlem_ratio_grouped(const Plan& P);
 recon_status_t build_exact_culling(Plan& P);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);
