@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     // small enough that a voxel rarely shows a second candidate that is not one
     const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;
     const float dz32 = 32.0f * G.vox[2];
+    const float nv_last = (float)(G.Nv - 1);
     for (int k0 = 0; k0 < G.Z; k0 += 32 * SLOTS) {
         const float fk0 = (float)(k0 + lane);
         const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
@@ -245,9 +246,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
             acc[s] = 0.0f;
             acc2[s * 32 + lane] = 0.0f;
         }
-        // the views' contributions to this chunk; FULL: every lane has SLOTS voxels
-        auto views = [&](auto full_tag) {
-            constexpr bool FULL = decltype(full_tag)::value;
+        {  // the views' contributions to this chunk
             for (unsigned vb = 0; vb < nview; vb += 32) {
                 const unsigned nb = min(32u, nview - vb);
                 if ((unsigned)lane < nb) {  // lane q sets up view vb + q
@@ -349,15 +348,16 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                             decltype(load_raw(col)) x[SLOTS];
 #pragma unroll
                             for (int s = 0; s < SLOTS; ++s) {
+                                // clamped to a detector row, so every load is in bounds: a row
+                                // that is no candidate gives L <= 0, and the sums of slots past
+                                // the volume's top are never written out
                                 const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
-                                const int a = max(0, __float2int_ru(f0));
-                                const bool in = (FULL || s < nslot) && a < G.Nv;
-                                vl[s] = min(a, G.Nv - 1);
-                                x[s] = 0;
-                                if (in) x[s] = load_raw(col + a + (a >> kRowGroupShift) * grow);
+                                const int a = __float2int_ru(fminf(fmaxf(f0, 0.0f), nv_last));
+                                vl[s] = a;
+                                x[s] = load_raw(col + a + (a >> kRowGroupShift) * grow);
                                 if (!SINGLE) {
                                     const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
-                                    if (in && (float)(a + 1) <= f1) more |= 1u << s;
+                                    if ((float)(a + 1) <= f1) more |= 1u << s;
                                 }
                             }
 #pragma unroll
@@ -390,11 +390,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                 }
                 __syncwarp();  // the next batch rewrites sv
             }
-        };
-        if (k0 + 32 * SLOTS <= G.Z)
-            views(std::true_type{});
-        else
-            views(std::false_type{});
+        }
 #pragma unroll
         for (int s = 0; s < SLOTS; ++s) {
             if (s >= nslot) continue;
