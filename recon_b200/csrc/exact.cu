@@ -201,6 +201,7 @@ struct GatherConst {
 struct GatherView {
     int u_lo, u_hi;
     float A[2], B[2], ca[2], cb[2];
+    unsigned single;  // bit sl: no voxel of the column has a second candidate row at u_lo + sl
 };
 
 template <bool UPDATE, class ST, int SLOTS>
@@ -265,6 +266,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                         umax = fmaxf(umax, uf);
                     }
                     GatherView V;
+                    V.single = 0u;
                     if (behind) {  // not for a volume in front of the source; stays exact anyway
                         V.u_lo = 0;
                         V.u_hi = G.Nu - 1;
@@ -283,6 +285,14 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                         V.B[sl] = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
                         V.ca[sl] = C.ez / (V.A[sl] + G.Rf);
                         V.cb[sl] = C.ez / (V.B[sl] + G.Rf);
+                        // a voxel's candidate interval [f0, f1] (row units) has a length
+                        // convex in its height, largest at the column's bottom or top voxel
+                        const float zb = G.P0[2], zt = G.P0[2] + (float)G.Z * G.vox[2];
+                        const float len_b = fmaxf((zb + G.vox[2]) * V.ca[sl], (zb + G.vox[2]) * V.cb[sl]) -
+                                            fminf(zb * V.ca[sl], zb * V.cb[sl]);
+                        const float len_t = fmaxf(zt * V.ca[sl], zt * V.cb[sl]) -
+                                            fminf((zt - G.vox[2]) * V.ca[sl], (zt - G.vox[2]) * V.cb[sl]);
+                        if (fmaxf(len_b, len_t) + (oz_hi - oz_lo) < 0.99f) V.single |= 1u << sl;
                     }
                     sv[lane] = V;
                 }
@@ -330,15 +340,8 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                         const float pa = dz32 * ca, pb = dz32 * cb;
                         const float P0a = fmaf(zl0, ca, oz_lo), P0b = fmaf(zl0, cb, oz_lo);
                         const float P1a = fmaf(zh0, ca, oz_hi), P1b = fmaf(zh0, cb, oz_hi);
-                        // The candidate interval's length f1 - f0 is convex in s (a max of
-                        // affine functions minus a min of them), so its largest value over
-                        // the slots is at s = 0 or s = SLOTS - 1: when both are under one
-                        // row, no voxel of the lane has a second candidate.
-                        const float s_last = (float)(SLOTS - 1);
-                        const float len = fmaxf(fmaxf(P1a, P1b) - fminf(P0a, P0b),
-                                                fmaxf(fmaf(s_last, pa, P1a), fmaf(s_last, pb, P1b)) -
-                                                    fminf(fmaf(s_last, pa, P0a), fmaf(s_last, pb, P0b)));
-                        const bool single = __all_sync(0xffffffffu, len < 0.999f);
+                        // no voxel of the column with a second candidate (set up per view)
+                        const bool single = sl < 2 && ((sv[q].single >> sl) & 1u);
                         // first candidate row of every voxel (loads issued together); a row that
                         // misses the voxel gives L <= 0 and adds nothing
                         unsigned more = 0u;
