@@ -1,7 +1,8 @@
 """ctypes wrapper for the checker libraries (test infrastructure only).
 
-Only tests/, ``__graft_entry__.smoke()`` and the cpu_baseline / reference legs
-of bench.py import this module.  It loads:
+Only tests/, ``__graft_entry__.smoke()``, the cpu_baseline / reference legs
+of bench.py and oracle/time_ref_gpu.py (a timing of the reference's own GPU
+build) import this module.  It loads:
 
 * ``oracle/liboracle.so``        -- the CPU restatement (siddon_oracle.c);
 * ``oracle/_ref/libref_cpu.so``  -- the reference's kernels built for the host;
