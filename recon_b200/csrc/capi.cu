@@ -432,7 +432,7 @@ recon_status_t recon_mlem_iteration(recon_plan_t P, const void* d_g, float* d_f,
     if (P->opt.bp == RECON_BP_VOXEL) {
         RB_CHECK(plain_fp_ratio(*P, d_f, static_cast<const float*>(d_g), static_cast<float*>(P->d_ratio), s));
         return voxel_bp(*P, static_cast<const float*>(P->d_ratio), 0, P->nviews, false, 0.0f, P->nviews,
-                        P->opt.voxel_mode, false, nullptr, P->d_sens, d_f, s);
+                        P->opt.voxel_mode, false, nullptr, P->d_sens, d_f, s, voxel_ratio_grouped(*P));
     }
     if (P->opt.arith == RECON_ARITH_COMPAT) return compat_mlem_iteration(*P, static_cast<const float*>(d_g), d_f, s);
     RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, s, 0, P->nviews));

@@ -121,11 +121,11 @@ __global__ void w_table_kernel(GeomD G, float* __restrict__ w, float* __restrict
 
 // MODE 0: out = projection (w * sum L_t * f).  MODE 1 (MLEM): out = w * ratio
 // with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input,
-// stored [view][v][u].  MODE 3: the same in the row-group layout
-// [view][v/8][u][v%8] (the gather back projector reads nearby rows of one
-// detector column; a CTA's 32 x 4 rays fill the halves of 32 row groups, which
-// the neighbouring row block completes).  MODE 2:
-// out = ratio (input of the voxel-driven back projector).
+// stored [view][v][u].  MODE 3 (4): w * ratio (the ratio) in the row-group layout
+// [view][v/16][u][v%16] (the gather back projectors read nearby rows of one
+// detector column; a CTA's 32 x 4 rays fill a quarter of 32 row groups, which the
+// neighbouring row blocks complete while the lines are in L2).  MODE 2: out =
+// ratio (input of the voxel-driven back projector), [view][v][u].
 template <bool KAHAN, int MODE, class GT, class OT>
 __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                   const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
@@ -153,10 +153,10 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
     } else {
         const float gv = load_val<GT>(g + n);
         const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-        if (MODE == 3)
+        if (MODE == 3 || MODE == 4)
             store_val<OT>(out + (size_t)(view - view0) * ((G.Nv + kRowGroup - 1) >> kRowGroupShift) * kRowGroup * G.Nu +
                               ((size_t)(v >> kRowGroupShift) * G.Nu + u) * kRowGroup + (v & (kRowGroup - 1)),
-                          ratio * w);
+                          MODE == 3 ? ratio * w : ratio);
         else
             store_val<OT>(out + n, MODE == 1 ? ratio * w : ratio);
     }
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
 // further ones into a shared-memory sum, and Ht = register + shared sum, so
 // the result is deterministic.
 //
-// Values are read in the row-group layout [view][v/8][u][v%8] (view_stride
+// Values are read in the row-group layout [view][v/16][u][v%16] (view_stride
 // elements per view; 0 for the weights w of the sensitivity).  UPDATE:
 // f = (sens != 0) ? f * Ht / sens : 0; otherwise vol = Ht.
 constexpr int kGatherWarps = 8;  // a kGatherTileX x (8 / kGatherTileX) tile of columns per CTA
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     }
 }
 
-// A sinogram [view][v][u] times w in the row-group layout [view][v/8][u][v%8]
+// A sinogram [view][v][u] times w in the row-group layout [view][v/16][u][v%16]
 // that the gather reads; rows past Nv are zero.  One thread per (u, row group)
 // of a view.
 __global__ void __launch_bounds__(128) to_row_groups_kernel(const float* __restrict__ in, const float* __restrict__ w,
@@ -731,7 +731,7 @@ static recon_status_t launch_fp(Plan& P, const float* vol, unsigned first, unsig
     const uint2* tiles;
     unsigned n_launch;
     ray_launch(P, P.fp_tiles, first, count, &grid, &tiles, &n_launch);
-    if (tiles && MODE != 1 && MODE != 3) RB_CUDA(cudaMemsetAsync(out, 0, (size_t)count * P.npix * sizeof(OT), s));
+    if (tiles && MODE != 1 && MODE != 3 && MODE != 4) RB_CUDA(cudaMemsetAsync(out, 0, (size_t)count * P.npix * sizeof(OT), s));
     if (n_launch == 0) return RECON_OK;
     RB_CHECK(exact_transpose(vol, P.d_vol_t, P.eg.X, P.eg.Y, P.eg.Z, s));
     const dim3 blk = fp_block();
@@ -847,6 +847,7 @@ recon_status_t exact_count(Plan& P, unsigned long long* out)
 
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s)
 {
+    if (voxel_ratio_grouped(P)) return launch_fp<4, float, float>(P, vol, 0u, P.nviews, g, ratio, s);
     return launch_fp<2, float, float>(P, vol, 0u, P.nviews, g, ratio, s);
 }
 
@@ -1023,7 +1024,7 @@ static recon_status_t ensure_row_groups(Plan& P, unsigned count)
     return RECON_OK;
 }
 
-// Elements per view in the row-group layout [v/8][u][v%8].
+// Elements per view in the row-group layout [v/16][u][v%16].
 size_t row_group_view(const Plan& P) { return (size_t)((P.eg.Nv + kRowGroup - 1) / kRowGroup) * kRowGroup * P.eg.Nu; }
 
 // The MLEM ratio is stored in the row-group layout when the gather back
@@ -1033,7 +1034,17 @@ bool mlem_ratio_grouped(const Plan& P)
     return P.bp_gather && P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_SIDDON;
 }
 
-size_t mlem_ratio_view(const Plan& P) { return mlem_ratio_grouped(P) ? row_group_view(P) : P.npix; }
+// The voxel-driven back projector's ratio (no w) is row-grouped too for EXACT
+// plans in GEOMETRIC mode (no detector tilt there), read by its gather kernel.
+bool voxel_ratio_grouped(const Plan& P)
+{
+    return P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_VOXEL && P.opt.voxel_mode == RECON_VOXEL_GEOMETRIC;
+}
+
+size_t mlem_ratio_view(const Plan& P)
+{
+    return (mlem_ratio_grouped(P) || voxel_ratio_grouped(P)) ? row_group_view(P) : P.npix;
+}
 
 recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, unsigned first, unsigned count,
                         bool scratch_slot, bool sens_mode, float* vol, const float* sens, float* f_update,

@@ -111,7 +111,7 @@ struct Plan {
     float2* d_cs = nullptr;    // [view] {cos, sin} of the view angle
     ZParam* d_zp = nullptr;    // [v]
     float* d_w = nullptr;      // [v][u] |p2-p1| / R
-    float* d_wq = nullptr;     // the same in the row-group layout [v/8][u][v%8]
+    float* d_wq = nullptr;     // the same in the row-group layout [v/16][u][v%16]
     float* d_rowgroups = nullptr;  // a sinogram in the row-group layout (gather back projector input)
     unsigned rowgroup_views = 0;   // views d_rowgroups holds
     bool bp_gather = false;    // Siddon back projection by the column gather (else ray-driven slabs)
@@ -194,7 +194,7 @@ recon_status_t compat_sensitivity(Plan& P, float* sens, cudaStream_t s);
 
 recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned count, bool scratch_slot,
                         float angle_scratch, unsigned Nproj, int mode, bool ones, float* vol_accum,
-                        const float* sens, float* f_update, cudaStream_t s);
+                        const float* sens, float* f_update, cudaStream_t s, bool rowgrouped = false);
 recon_status_t plain_fp_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
 recon_status_t compat_fp_ratio_all(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
@@ -210,9 +210,11 @@ bool exact_bp_gather_suits(const Plan& P);
 recon_status_t march_fp_view(Plan& P, const float* vol, float angle_deg, int mode, float* img, cudaStream_t s);
 int exact_bp_gather_max_rows();
 size_t mlem_ratio_view(const Plan& P);
+bool voxel_ratio_grouped(const Plan& P);
+int gather_slots(int Z);
 // Row-group layout of sinograms read by the gather back projector:
 // [view][v / kRowGroup][u][v % kRowGroup].
-constexpr int kRowGroup = 8, kRowGroupShift = 3;
+constexpr int kRowGroup = 16, kRowGroupShift = 4;
 size_t row_group_view(const Plan& P);
 bool mlem_ratio_grouped(const Plan& P);
 recon_status_t build_exact_culling(Plan& P);

@@ -228,6 +228,123 @@ __global__ void __launch_bounds__(128) bp_column_kernel(VGeom G, const float* __
     }
 }
 
+// GEOMETRIC mode without tilt, gathered per column by a warp (the layout of
+// the Siddon gather back projector, exact.cu): lane l owns the voxels
+// k0 + l + 32 s (s < SLOTS) of a column chunk and keeps their sums in
+// registers.  Per view the column's detector column u_pix and the row of its
+// bottom voxel centre vA (with the row step per voxel vB) are set up 32 views
+// at a time, one per lane, in shared memory; then every lane samples its
+// voxels' rows v = vA + k vB with the same bilinear arithmetic as
+// bp_column_kernel.  The view images are read in the row-group layout
+// [view][v/16][u][v%16] (view_stride elements per view), so one tap of all 32
+// lanes (about 26 consecutive rows of one detector column) lies in one or two
+// 128-byte lines.  The taps of four voxels are loaded before any is used.  MODE
+// as in bp_kernel; MODE 1 reads nothing.
+constexpr int kVoxelWarps = 8;  // a 4 x 2 tile of columns per CTA
+
+template <int MODE, int SLOTS>
+__global__ void __launch_bounds__(kVoxelWarps * 32, 3) bp_gather_kernel(VGeom G, const float* __restrict__ angles,
+                                                                       unsigned view0, unsigned nview, unsigned Nproj,
+                                                                       const float* __restrict__ rg, size_t view_stride,
+                                                                       float* __restrict__ vol,
+                                                                       const float* __restrict__ sens)
+{
+    __shared__ float4 sview[kVoxelWarps][32];  // per view: {u_pix, vA, vB, -}
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int x = blockIdx.x * 4 + (warp & 3), y = blockIdx.y * 2 + (warp >> 2);
+    if (x >= G.X || y >= G.Y) return;  // whole warps; no block barrier
+    float4* sv = sview[warp];
+    const size_t plane = (size_t)G.X * G.Y;
+    const float xo = center((float)G.X, G.vox[0], 1.0f, x);
+    const float yo = center((float)G.Y, G.vox[1], 1.0f, y);
+    const float inv_du = 1.0f / (G.du_mm * G.M), inv_dv = 1.0f / (G.dv_mm * G.M);
+    const float cu = (float)(G.Nu - 1) * 0.5f, cv = (float)(G.Nv - 1) * 0.5f;
+    const float umax = (float)(G.Nu - 1), vmax = (float)(G.Nv - 1);
+    const float inv_n = 1.0f / (float)Nproj;
+    const int grow = kRowGroup * G.Nu - kRowGroup;  // row v of a detector column: v + (v / kRowGroup) * grow
+    for (int k0 = 0; k0 < G.Z; k0 += 32 * SLOTS) {
+        const float z0 = center((float)G.Z, G.vox[2], 1.0f, k0);
+        float acc[SLOTS];
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+            const int k = k0 + lane + 32 * s;
+            acc[s] = (MODE == 0 && k < G.Z) ? vol[(size_t)x + (size_t)y * G.X + (size_t)k * plane] : 0.0f;
+        }
+        for (unsigned vb = 0; vb < nview; vb += 32) {
+            const unsigned nb = min(32u, nview - vb);
+            if ((unsigned)lane < nb) {
+                const float alpha = angles[view0 + vb + lane];
+                const float c = cospif(alpha / 180.0f), sn = sinpif(alpha / 180.0f);
+                const float xa = xo * c - yo * sn;
+                const float ya = xo * sn + yo * c;
+                const float inv = 1.0f / (ya + G.Rf);
+                sv[lane] = make_float4((G.Ry * xa * inv - G.Dx) * inv_du + cu, (G.Ry * inv * z0 - G.Dz) * inv_dv + cv,
+                                       G.Ry * inv * G.vox[2] * inv_dv, 0.0f);
+            }
+            __syncwarp();
+            for (unsigned q = 0; q < nb; ++q) {
+                const float4 V = sv[q];
+                const float u_pix = V.x;
+                if (!(u_pix >= 0.0f && u_pix <= umax)) continue;
+                const int ui = min(max((int)floorf(u_pix), 0), G.Nu - 2);
+                const float uw = u_pix - (float)ui;
+                const float* __restrict__ col = rg + (size_t)(vb + q) * view_stride + (size_t)ui * kRowGroup;
+                const float vbase = fmaf((float)lane, V.z, V.y);
+                // taps of PH voxels at a time, loaded before any is used: rows are
+                // clamped to the image, so every address is valid, and voxels whose
+                // row lies outside the image are dropped when adding
+                constexpr int PH = SLOTS < 4 ? SLOTS : 4;
+#pragma unroll
+                for (int p0 = 0; p0 < SLOTS; p0 += PH) {
+                    float t00[PH], t10[PH], t01[PH], t11[PH], vw[PH];
+                    bool ok[PH];
+#pragma unroll
+                    for (int jj = 0; jj < PH; ++jj) {
+                        const int s = p0 + jj;
+                        if (s >= SLOTS) break;
+                        const float v_pix = fmaf((float)(32 * s), V.z, vbase);
+                        ok[jj] = v_pix >= 0.0f && v_pix <= vmax;
+                        const int vj = min(max((int)floorf(v_pix), 0), G.Nv - 2);
+                        vw[jj] = v_pix - (float)vj;
+                        if (MODE != 1) {
+                            const float* r0 = col + vj + (vj >> kRowGroupShift) * grow;
+                            const float* r1 = col + (vj + 1) + ((vj + 1) >> kRowGroupShift) * grow;
+                            t00[jj] = __ldg(r0);
+                            t10[jj] = __ldg(r0 + kRowGroup);
+                            t01[jj] = __ldg(r1);
+                            t11[jj] = __ldg(r1 + kRowGroup);
+                        }
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < PH; ++jj) {
+                        const int s = p0 + jj;
+                        if (s >= SLOTS) break;
+                        if (!ok[jj]) continue;
+                        float val = 1.0f;
+                        if (MODE != 1)
+                            val = (t00[jj] * (1.0f - uw) + t10[jj] * uw) * (1.0f - vw[jj]) +
+                                  (t01[jj] * (1.0f - uw) + t11[jj] * uw) * vw[jj];
+                        acc[s] = fmaf(val, inv_n, acc[s]);
+                    }
+                }
+            }
+            __syncwarp();  // the next batch rewrites sv
+        }
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+            const int k = k0 + lane + 32 * s;
+            if (k >= G.Z) continue;
+            const size_t n = (size_t)x + (size_t)y * G.X + (size_t)k * plane;
+            if (MODE == 2) {
+                const float svv = sens[n];
+                vol[n] = (svv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[n], acc[s]), svv) : 0.0f;
+            } else {
+                vol[n] = acc[s];
+            }
+        }
+    }
+}
+
 }  // namespace voxel
 
 // ---- host side ----------------------------------------------------------------------
@@ -305,10 +422,12 @@ static void release_textures(TexCache& c)
 
 void release_plan_textures(Plan* P) { release_textures(P->tex); }
 
+// rowgrouped: sino is in the row-group layout (the MLEM ratio of an EXACT
+// plan with this back projector), else [view][v][u].
 template <int VMODE, int MODE>
 static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angles, unsigned first, unsigned count,
                                    unsigned Nproj, float* vol, const float* sens, bool cache_textures,
-                                   cudaStream_t s)
+                                   bool rowgrouped, cudaStream_t s)
 {
     voxel::VGeom G = vgeom(P);
     dim3 blk(32, 4, 1), grid((G.X + 31) / 32, (G.Y + 3) / 4, G.Z);
@@ -316,7 +435,7 @@ static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angl
     cudaTextureObject_t* d_handles = nullptr;
     std::vector<cudaTextureObject_t> local;
     cudaTextureObject_t* d_local = nullptr;
-    if (VMODE == RECON_VOXEL_GEOMETRIC && MODE != 1 && sino) {
+    if (VMODE == RECON_VOXEL_GEOMETRIC && MODE != 1 && sino && !rowgrouped) {
         if (cache_textures) {
             TexCache& c = P.tex;
             if (c.base != sino || c.count != count) {
@@ -342,6 +461,28 @@ static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angl
         }
     }
     const bool untilted = P.geom.cal.xangle == 0.0f && P.geom.cal.yangle == 0.0f && P.geom.cal.zangle == 0.0f;
+    if (VMODE == RECON_VOXEL_GEOMETRIC && untilted && (MODE == 1 || rowgrouped)) {
+        const dim3 ggrid((G.X + 3) / 4, (G.Y + 1) / 2);
+        const size_t stride = row_group_view(P);
+        switch (gather_slots(G.Z)) {
+#define RB_VOXEL_SLOTS(n)                                                                                          \
+    case n:                                                                                                        \
+        voxel::bp_gather_kernel<MODE, n><<<ggrid, voxel::kVoxelWarps * 32, 0, s>>>(G, angles, first, count, Nproj, \
+                                                                                  sino, stride, vol, sens);        \
+        break
+            RB_VOXEL_SLOTS(1);
+            RB_VOXEL_SLOTS(2);
+            RB_VOXEL_SLOTS(3);
+            RB_VOXEL_SLOTS(4);
+            RB_VOXEL_SLOTS(5);
+            RB_VOXEL_SLOTS(6);
+            RB_VOXEL_SLOTS(7);
+            default: RB_VOXEL_SLOTS(8);
+#undef RB_VOXEL_SLOTS
+        }
+        RB_CUDA(cudaGetLastError());
+        return RECON_OK;
+    }
     if (VMODE == RECON_VOXEL_GEOMETRIC && untilted) {
         constexpr int ZC = 16;
         const dim3 cgrid((G.X + 31) / 32, (G.Y + 3) / 4, (G.Z + ZC - 1) / ZC);
@@ -373,7 +514,7 @@ __global__ void voxel_set_angle_kernel(float* p, float v) { *p = v; }
 
 recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned count, bool scratch_slot,
                         float angle_scratch, unsigned Nproj, int mode, bool ones, float* vol_accum,
-                        const float* sens, float* f_update, cudaStream_t s)
+                        const float* sens, float* f_update, cudaStream_t s, bool rowgrouped)
 {
     if (scratch_slot) {
         voxel_set_angle_kernel<<<1, 1, 0, s>>>(P.d_angles + P.nviews, angle_scratch);
@@ -384,20 +525,20 @@ recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned cou
     const bool cache = !scratch_slot;
     if (ones) {
         return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 1>(P, nullptr, P.d_angles, first, count, Nproj, vol_accum,
-                                                             nullptr, false, s)
+                                                             nullptr, false, false, s)
                    : launch_voxel<RECON_VOXEL_GEOMETRIC, 1>(P, nullptr, P.d_angles, first, count, Nproj, vol_accum,
-                                                             nullptr, false, s);
+                                                             nullptr, false, false, s);
     }
     if (f_update) {
         return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 2>(P, sino, P.d_angles, first, count, Nproj, f_update, sens,
-                                                             cache, s)
+                                                             cache, rowgrouped, s)
                    : launch_voxel<RECON_VOXEL_GEOMETRIC, 2>(P, sino, P.d_angles, first, count, Nproj, f_update, sens,
-                                                             cache, s);
+                                                             cache, rowgrouped, s);
     }
     return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 0>(P, sino, P.d_angles, first, count, Nproj, vol_accum, nullptr,
-                                                         cache, s)
+                                                         cache, rowgrouped, s)
                : launch_voxel<RECON_VOXEL_GEOMETRIC, 0>(P, sino, P.d_angles, first, count, Nproj, vol_accum, nullptr,
-                                                         cache, s);
+                                                         cache, rowgrouped, s);
 }
 
 }  // namespace rb
