@@ -235,7 +235,7 @@ def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int
 
 def voxel_leg(cfg, g, steps: int, warmup: int, device_index: int):
     """The same MLEM iteration with the voxel-driven back projector
-    (texture point fetches + FP32 bilinear weights, geometric mode) in place
+    (geometric mode: FP32 bilinear taps, gathered per voxel column) in place
     of the Siddon one: Siddon forward projection with the plain ratio, then
     the voxel-driven back projection with the update fused in."""
     import torch
@@ -256,7 +256,7 @@ def voxel_leg(cfg, g, steps: int, warmup: int, device_index: int):
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / steps
     return {"value": 1e3 / ms, "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
-            "back_projector": "voxel-driven, texture point fetch + FP32 bilinear (geometric mode)"}
+            "back_projector": "voxel-driven, FP32 bilinear taps gathered per voxel column (geometric mode)"}
 
 
 def ref_view_seconds(R, O, geo, cfg, view, steps, f, gview, ht):
