@@ -25,6 +25,7 @@ BP_SIDDON, BP_VOXEL = 0, 1
 VOXEL_REFERENCE, VOXEL_GEOMETRIC = 0, 1
 SIDDON_BP_AUTO, SIDDON_BP_GATHER, SIDDON_BP_RAY = 0, 1, 2
 NOALLOC_MAX_VOXELS = 2097152  # RECON_NOALLOC_MAX_VOXELS
+ABI_VERSION = 2  # RECON_B200_ABI_VERSION: the layout of the structures above
 
 
 class ReconError(RuntimeError):

@@ -34,7 +34,9 @@ def test_exports_every_declared_function():
     for name in declared:
         assert hasattr(lib, name), name
     assert sorted(L.exported_symbols()) == declared
-    assert lib.recon_abi_version() == 2
+    assert lib.recon_abi_version() == L.ABI_VERSION
+    header = open(os.path.join(ROOT, "include", "recon_b200.h")).read()
+    assert f"#define RECON_B200_ABI_VERSION {L.ABI_VERSION}\n" in header
 
 
 def test_default_options():
