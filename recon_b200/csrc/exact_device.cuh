@@ -136,7 +136,7 @@ __device__ __forceinline__ float fp_ray_sum(const ExactGeom& G, const float4 T, 
         const unsigned vmax = (unsigned)(G.X * G.Y * G.Z - 1);
         int idx = ix * V.ux + iy * V.uy + iz * G.X * G.Y;
         float cur = t_in, comp = 0.0f;
-#pragma unroll 2
+#pragma unroll 4  // 2 and 8 measured 2 % slower, 3 slower still
         for (int s = 0; s < nsteps; ++s) {
             const float m = fminf(tx, fminf(ty, tz));
             const float fv = __ldg(vol + min((unsigned)idx, vmax));
