@@ -236,7 +236,6 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     // small enough that a voxel rarely shows a second candidate that is not one
     const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;
     const float dz32 = 32.0f * G.vox[2];
-    const float nv_last = (float)(G.Nv - 1);
     for (int k0 = 0; k0 < G.Z; k0 += 32 * SLOTS) {
         const float fk0 = (float)(k0 + lane);
         const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
@@ -353,9 +352,11 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                             for (int s = 0; s < SLOTS; ++s) {
                                 // clamped to a detector row, so every load is in bounds: a row
                                 // that is no candidate gives L <= 0, and the sums of slots past
-                                // the volume's top are never written out
+                                // the volume's top are never written out.  The conversion to
+                                // unsigned saturates (negative rows and NaN give 0), which leaves
+                                // one min for the clamp
                                 const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
-                                const int a = __float2int_ru(fminf(fmaxf(f0, 0.0f), nv_last));
+                                const int a = (int)min(__float2uint_ru(f0), (unsigned)G.Nv - 1u);
                                 vl[s] = a;
                                 x[s] = load_raw(col + a + (a >> kRowGroupShift) * grow);
                                 if (!SINGLE) {

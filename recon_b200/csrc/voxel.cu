@@ -304,7 +304,8 @@ __global__ void __launch_bounds__(kVoxelWarps * 32, 3) bp_gather_kernel(VGeom G,
                         if (s >= SLOTS) break;
                         const float v_pix = fmaf((float)(32 * s), V.z, vbase);
                         ok[jj] = v_pix >= 0.0f && v_pix <= vmax;
-                        const int vj = min(max((int)floorf(v_pix), 0), G.Nv - 2);
+                        // floor, saturated at 0 by the conversion to unsigned (NaN gives 0)
+                        const int vj = (int)min(__float2uint_rd(v_pix), (unsigned)G.Nv - 2u);
                         vw[jj] = v_pix - (float)vj;
                         if (MODE != 1) {
                             const float* r0 = col + vj + (vj >> kRowGroupShift) * grow;
