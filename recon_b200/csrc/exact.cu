@@ -237,6 +237,15 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;
     const float dz32 = 32.0f * G.vox[2];
     for (int k0 = 0; k0 < G.Z; k0 += 32 * SLOTS) {
+        // Slots below the source plane z = 0 (voxels k < Z/2, the volume being centred)
+        // when that is the same count for every lane, else -1.  The bound f0 of voxel k
+        // is min over the piece of z_k * c and f1 the max of z_k+1 * c: c = ez / (depth)
+        // is larger at the piece's near end, so the near end gives f0 below z = 0 and
+        // f1 above, the far end the others.  Rounding can make the other end's value
+        // pass by an ulp, which moves a bound only where it lies a row's 0.002 margin
+        // away from the voxel: the row it adds or drops has no length there.
+        const int rel = (G.Z + 1) / 2 - k0;
+        const int split = rel <= 0 ? 0 : (rel >= 32 * SLOTS ? SLOTS : (rel % 32 == 0 ? rel / 32 : -1));
         const float fk0 = (float)(k0 + lane);
         const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
         const int nslot = min(SLOTS, max(0, (G.Z - k0 - lane + 31) / 32));
@@ -344,33 +353,50 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                         // first candidate row of every voxel (loads issued together); a row that
                         // misses the voxel gives L <= 0 and adds nothing
                         unsigned more = 0u;
-                        auto first_rows = [&](auto single_tag) {
+                        auto first_rows = [&](auto single_tag, auto split_tag) {
                             constexpr bool SINGLE = decltype(single_tag)::value;
+                            constexpr int SPLIT = decltype(split_tag)::value;
                             int vl[SLOTS];
                             decltype(load_raw(col)) x[SLOTS];
 #pragma unroll
                             for (int s = 0; s < SLOTS; ++s) {
+                                // the lower of the two bounds: the piece's near end (a) for
+                                // voxels below the source plane, its far end (b) above it,
+                                // where the slot is on one side for every lane (SPLIT >= 0)
+                                const float f0 = SPLIT < 0 ? fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b))
+                                                           : (s < SPLIT ? fmaf((float)s, pa, P0a) : fmaf((float)s, pb, P0b));
                                 // clamped to a detector row, so every load is in bounds: a row
                                 // that is no candidate gives L <= 0, and the sums of slots past
                                 // the volume's top are never written out.  The conversion to
                                 // unsigned saturates (negative rows and NaN give 0), which leaves
                                 // one min for the clamp
-                                const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
                                 const int a = (int)min(__float2uint_ru(f0), (unsigned)G.Nv - 1u);
                                 vl[s] = a;
                                 x[s] = load_raw(col + a + (a >> kRowGroupShift) * grow);
-                                if (!SINGLE) {
-                                    const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                                if (!SINGLE) {  // the higher top bound: far end below z = 0, near end above
+                                    const float f1 =
+                                        SPLIT < 0 ? fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b))
+                                                  : (s < SPLIT ? fmaf((float)s, pb, P1b) : fmaf((float)s, pa, P1a));
                                     if ((float)(a + 1) <= f1) more |= 1u << s;
                                 }
                             }
 #pragma unroll
                             for (int s = 0; s < SLOTS; ++s) add(s, vl[s], widen(x[s]));
                         };
+                        auto rows = [&](auto single_tag) {
+                            if (SLOTS == 8 && split == 0)
+                                first_rows(single_tag, std::integral_constant<int, 0>{});
+                            else if (SLOTS == 8 && split == SLOTS / 2)
+                                first_rows(single_tag, std::integral_constant<int, SLOTS / 2>{});
+                            else if (SLOTS == 8 && split == SLOTS)
+                                first_rows(single_tag, std::integral_constant<int, SLOTS>{});
+                            else
+                                first_rows(single_tag, std::integral_constant<int, -1>{});
+                        };
                         if (single)
-                            first_rows(std::true_type{});
+                            rows(std::true_type{});
                         else
-                            first_rows(std::false_type{});
+                            rows(std::false_type{});
                         // further candidates (rare): summed apart, in shared memory
                         if (__any_sync(0xffffffffu, more != 0u)) {
                             for (unsigned m = more; m != 0u; m &= m - 1u) {
