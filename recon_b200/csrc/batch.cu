@@ -221,7 +221,9 @@ recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const re
         b->events.push_back(e);
     }
     RB_CUDA(cudaEventCreateWithFlags(&b->sync, cudaEventDisableTiming));
-    RB_CUDA(cudaDeviceSynchronize());
+    // plans are set up on the legacy stream; a device-wide synchronisation here
+    // would invalidate another thread's batch graph capture
+    RB_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
     *out = b.release();
     return RECON_OK;
 }

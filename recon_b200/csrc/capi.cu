@@ -296,7 +296,10 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CUDA(cudaMemset(P->d_fix, 0, P->nvox * sizeof(unsigned long long)));
             RB_CHECK(build_compat_tables(*P, 0));
         }
-        RB_CUDA(cudaDeviceSynchronize());
+        // the set-up ran on the legacy stream; waiting for that stream alone (not the
+        // device) leaves alone other threads' graph captures, which a device-wide
+        // synchronisation would invalidate
+        RB_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
         return RECON_OK;
     }();
     if (st != RECON_OK) {

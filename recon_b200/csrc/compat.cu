@@ -584,7 +584,7 @@ recon_status_t compat_setup_dump(Plan& P, float angle, float* h[10], unsigned* l
     compat::setup_dump_kernel<<<ray_grid(P, 1), ray_block(), 0, s>>>(P.cg, angle, amin, amax, d12, mask, ai, af, da,
                                                                       p1, p2, dindex);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
     void* dev[10] = {amin, amax, d12, mask, ai, af, da, p1, p2, dindex};
     size_t sz[10] = {n * 4, n * 4, n * 4, n * 4, n * 12, n * 12, n * 12, n * 12, n * 12, n * 4};
     for (int k = 0; k < 10 && e == cudaSuccess; ++k) e = cudaMemcpy(h[k], dev[k], sz[k], cudaMemcpyDeviceToHost);
@@ -612,7 +612,7 @@ recon_status_t compat_trace(Plan& P, float angle, int nrays, const int* rays, in
     if (e == cudaSuccess && nrays > 0) {
         compat::trace_kernel<<<(nrays + 127) / 128, 128>>>(P.cg, angle, loopN, nrays, d_rays, cap, d_idx, d_len);
         e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
         if (e == cudaSuccess) e = cudaMemcpy(idx, d_idx, sizeof(int) * (size_t)nrays * cap, cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaMemcpy(len, d_len, sizeof(float) * (size_t)nrays * cap, cudaMemcpyDeviceToHost);
     }
