@@ -404,13 +404,14 @@ def main():
     npix = P.nu * P.nv
     nvox = f.numel()
     # kernels per step: transpose + forward; the gather back projector is one
-    # kernel, the ray-driven one maxabs + (ray + finish) per z-slab (both int64
-    # accumulators of a slab in 64 MiB); at N > 1 a separate update
+    # kernel after the ratio's transpose into detector columns, the ray-driven one
+    # maxabs + (ray + finish) per z-slab (both int64 accumulators of a slab in
+    # 64 MiB); at N > 1 a separate update
     gather = P.siddon_bp == SIDDON_BP_GATHER
     Z, Y, X = P.shape_vol
     depth = max(1, min(Z, (64 << 20) // (X * Y * 16)))
     slabs = -(-Z // depth)
-    bp_launches = 1 if gather else 1 + 2 * slabs
+    bp_launches = 2 if gather else 1 + 2 * slabs
 
     def iteration(ev=None):
         if world == 1:

@@ -183,12 +183,17 @@ recon_status_t ensure_mlem_buffers(Plan& P)
     if (!P.d_ratio) {
         const size_t es = (P.opt.sino == RECON_SINO_BF16) ? 2 : 4;
         const bool per_view = (P.opt.arith == RECON_ARITH_COMPAT) && (P.opt.bp == RECON_BP_SIDDON);
-        const size_t n = per_view ? P.npix : (size_t)P.nviews * mlem_ratio_view(P);
+        const size_t n = per_view ? P.npix : (size_t)P.nviews * P.npix;
         char* q = nullptr;
         RB_CHECK(P.alloc(&q, n * es, "ratio sinogram"));
         // zero outside the ray blocks the forward projector writes (EXACT culling)
         RB_CUDA(cudaMemset(q, 0, n * es));
         P.d_ratio = q;
+        if (P.opt.arith == RECON_ARITH_EXACT && (mlem_ratio_in_columns(P) || voxel_ratio_in_columns(P))) {
+            RB_CHECK(P.alloc(&q, n * es, "ratio sinogram (staging)"));
+            RB_CUDA(cudaMemset(q, 0, n * es));
+            P.d_ratio_rm = q;
+        }
     }
     return RECON_OK;
 }
@@ -274,8 +279,8 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_w, P->npix, "ray weights"));
             P->bp_gather = opt.siddon_bp == RECON_SIDDON_BP_GATHER ||
                            (opt.siddon_bp == RECON_SIDDON_BP_AUTO && exact_bp_gather_suits(*P));
-            RB_CHECK(P->alloc(&P->d_wq, row_group_view(*P), "ray weights (row groups)"));
-            RB_CUDA(cudaMemset(P->d_wq, 0, row_group_view(*P) * sizeof(float)));
+            RB_CHECK(P->alloc(&P->d_wq, P->npix, "ray weights (detector columns)"));
+            RB_CUDA(cudaMemset(P->d_wq, 0, P->npix * sizeof(float)));
             if (P->bp_gather && P->eg.Nv > exact_bp_gather_max_rows())
                 return fail(RECON_ERR_UNSUPPORTED, "the gather back projector takes at most 12288 detector rows");
             RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
@@ -435,7 +440,7 @@ recon_status_t recon_mlem_iteration(recon_plan_t P, const void* d_g, float* d_f,
     if (P->opt.bp == RECON_BP_VOXEL) {
         RB_CHECK(plain_fp_ratio(*P, d_f, static_cast<const float*>(d_g), static_cast<float*>(P->d_ratio), s));
         return voxel_bp(*P, static_cast<const float*>(P->d_ratio), 0, P->nviews, false, 0.0f, P->nviews,
-                        P->opt.voxel_mode, false, nullptr, P->d_sens, d_f, s, voxel_ratio_grouped(*P));
+                        P->opt.voxel_mode, false, nullptr, P->d_sens, d_f, s, voxel_ratio_in_columns(*P));
     }
     if (P->opt.arith == RECON_ARITH_COMPAT) return compat_mlem_iteration(*P, static_cast<const float*>(d_g), d_f, s);
     RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, s, 0, P->nviews));
@@ -470,7 +475,7 @@ recon_status_t recon_mlem_backward(recon_plan_t P, unsigned first, unsigned coun
     cudaStream_t s = as_stream(stream);
     if (count == 0) return launch_fill(d_ht, 0.0f, P->nvox, s);
     const size_t es = P->opt.sino == RECON_SINO_BF16 ? 2 : 4;
-    const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * mlem_ratio_view(*P) * es;
+    const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * P->npix * es;
     return exact_bp(*P, r, true, P->opt.sino == RECON_SINO_BF16, first, count, false, false, d_ht, nullptr, nullptr,
                     s);
 }
@@ -528,7 +533,7 @@ recon_status_t recon_osem(recon_plan_t P, const void* d_g, unsigned iters, unsig
         for (unsigned k = 0; k < n_subsets; ++k) {
             const unsigned first = k * n;
             RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, s, first, n));
-            const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * mlem_ratio_view(*P) * es;
+            const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * P->npix * es;
             RB_CHECK(exact_bp(*P, r, true, bf16, first, n, false, false, nullptr,
                               P->d_osem_sens + (size_t)k * P->nvox, d_f, s));
         }

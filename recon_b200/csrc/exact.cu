@@ -105,8 +105,8 @@ __global__ void z_table_kernel(GeomD G, ZParam* __restrict__ zp)
     zp[v] = z;
 }
 
-// w = |p2 - p1| / R per ray, stored [v][u] (w) and in the row-group layout
-// [v/4][u][v%4] (wq)
+// w = |p2 - p1| / R per ray, stored [v][u] (w) and in the detector-column layout
+// [u][v] (wq)
 __global__ void w_table_kernel(GeomD G, float* __restrict__ w, float* __restrict__ wq)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -116,16 +116,15 @@ __global__ void w_table_kernel(GeomD G, float* __restrict__ w, float* __restrict
     const double det_z = G.R / G.Ry * (pixel_center_d(G.Nv, G.dv, v) + G.Dz);
     const float wv = (float)(sqrt(det_x * det_x + G.R * G.R + det_z * det_z) / G.R);
     w[(size_t)v * G.Nu + u] = wv;
-    wq[((size_t)(v >> kRowGroupShift) * G.Nu + u) * kRowGroup + (v & (kRowGroup - 1))] = wv;
+    wq[(size_t)u * G.Nv + v] = wv;
 }
 
 // MODE 0: out = projection (w * sum L_t * f).  MODE 1 (MLEM): out = w * ratio
-// with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input,
-// stored [view][v][u].  MODE 3 (4): w * ratio (the ratio) in the row-group layout
-// [view][v/16][u][v%16] (the gather back projectors read nearby rows of one
-// detector column; a CTA's 32 x 4 rays fill a quarter of 32 row groups, which the
-// neighbouring row blocks complete while the lines are in L2).  MODE 2: out =
-// ratio (input of the voxel-driven back projector), [view][v][u].
+// with ratio = g / Hf (0 where Hf == 0), the Siddon back projector's input.
+// MODE 2: out = ratio (input of the voxel-driven back projector).  All stored
+// [view][v][u], so that a warp's 32 rays (adjacent detector columns) store 128
+// contiguous bytes; the gather back projectors read a transposed copy
+// (to_columns_kernel).
 template <bool KAHAN, int MODE, class GT, class OT>
 __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                   const int2* __restrict__ kxy, const ZParam* __restrict__ zp,
@@ -153,12 +152,7 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
     } else {
         const float gv = load_val<GT>(g + n);
         const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-        if (MODE == 3 || MODE == 4)
-            store_val<OT>(out + (size_t)(view - view0) * ((G.Nv + kRowGroup - 1) >> kRowGroupShift) * kRowGroup * G.Nu +
-                              ((size_t)(v >> kRowGroupShift) * G.Nu + u) * kRowGroup + (v & (kRowGroup - 1)),
-                          MODE == 3 ? ratio * w : ratio);
-        else
-            store_val<OT>(out + n, MODE == 1 ? ratio * w : ratio);
+        store_val<OT>(out + n, MODE == 1 ? ratio * w : ratio);
     }
 }
 
@@ -182,8 +176,10 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
 // further ones into a shared-memory sum, and Ht = register + shared sum, so
 // the result is deterministic.
 //
-// Values are read in the row-group layout [view][v/16][u][v%16] (view_stride
-// elements per view; 0 for the weights w of the sensitivity).  UPDATE:
+// Values are read in the detector-column layout [view][u][v] (view_stride
+// elements per view; 0 for the weights w of the sensitivity): a warp's loads of
+// nearby rows of one detector column fall in one or two 128-byte lines, and a
+// row's element is one add from its column.  UPDATE:
 // f = (sens != 0) ? f * Ht / sens : 0; otherwise vol = Ht.
 constexpr int kGatherWarps = 8;  // a kGatherTileX x (8 / kGatherTileX) tile of columns per CTA
 constexpr int kGatherTileX = 4;
@@ -230,7 +226,6 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
     const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
     const size_t plane = (size_t)G.X * G.Y;
-    const int grow = kRowGroup * G.Nu - kRowGroup;  // element of row v in a detector column: v + (v / kRowGroup) * grow
     // candidate rows are widened by 0.002 row on either side: about ten times the
     // FP32 error of the row bounds (values of a few hundred rows, a few roundings),
     // small enough that a voxel rarely shows a second candidate that is not one
@@ -328,7 +323,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                             cb = C.ez / (B + G.Rf);
                         }
                         if (!(A < B)) continue;
-                        const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * kRowGroup;
+                        const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * G.Nv;
                         auto add = [&](int s, int v, float x) {
                             const float4 zr = szq[v];
                             const float t = fk0 + (float)(32 * s);
@@ -340,7 +335,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
 #pragma unroll
                             for (int s = 0; s < SLOTS; ++s)
                                 if (s < nslot)
-                                    for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v + (v >> kRowGroupShift) * grow));
+                                    for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v));
                             continue;
                         }
                         // row bounds of slot s: f0 = min over the piece of the voxel's bottom
@@ -372,7 +367,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                                 // one min for the clamp
                                 const int a = (int)min(__float2uint_ru(f0), (unsigned)G.Nv - 1u);
                                 vl[s] = a;
-                                x[s] = load_raw(col + a + (a >> kRowGroupShift) * grow);
+                                x[s] = load_raw(col + a);
                                 if (!SINGLE) {  // the higher top bound: far end below z = 0, near end above
                                     const float f1 =
                                         SPLIT < 0 ? fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b))
@@ -411,7 +406,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                                     const float4 zr = szq[v];
                                     const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
                                     const float L = fminf(B, hi) - fmaxf(A, lo);
-                                    if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v + (v >> kRowGroupShift) * grow), sum);
+                                    if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v), sum);
                                 }
                                 acc2[s * 32 + lane] = sum;
                             }
@@ -436,26 +431,37 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     }
 }
 
-// A sinogram [view][v][u] times w in the row-group layout [view][v/16][u][v%16]
-// that the gather reads; rows past Nv are zero.  One thread per (u, row group)
-// of a view.
-__global__ void __launch_bounds__(128) to_row_groups_kernel(const float* __restrict__ in, const float* __restrict__ w,
-                                                           int Nu, int Nv, float4* __restrict__ out)
+// A sinogram [view][v][u] (times w when w is given) into the detector-column
+// layout [view][u][v] that the gather back projectors read: 32x32 (u, v) tiles
+// through shared memory, read and written along rows of 128 bytes.  With rect
+// (per view {u_min, u_max, v_min, v_max}), tiles wholly outside a view's
+// rectangle are skipped: the MLEM ratio is zero there in both layouts.
+template <class T>
+__global__ void __launch_bounds__(256) to_columns_kernel(const T* __restrict__ in, const float* __restrict__ w, int Nu,
+                                                         int Nv, const int4* __restrict__ rect, T* __restrict__ out)
 {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int q = blockIdx.y;
+    __shared__ T tile[32][33];
     const size_t view = blockIdx.z;
-    if (u >= Nu) return;
-    float r[kRowGroup];
-#pragma unroll
-    for (int c = 0; c < kRowGroup; ++c) {
-        const int v = kRowGroup * q + c;
-        r[c] = 0.0f;
-        if (v < Nv) r[c] = __ldg(in + (view * Nv + v) * Nu + u) * __ldg(w + (size_t)v * Nu + u);
+    const int u0 = blockIdx.x * 32, v0 = blockIdx.y * 32;
+    if (rect) {  // the same for the whole block: no barrier is skipped by part of it
+        const int4 r = rect[view];
+        if (u0 > r.y || u0 + 31 < r.x || v0 > r.w || v0 + 31 < r.z) return;
     }
-    float4* o = out + ((view * gridDim.y + q) * Nu + u) * (kRowGroup / 4);
-#pragma unroll
-    for (int c = 0; c < kRowGroup / 4; ++c) o[c] = make_float4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+    const T* __restrict__ src = in + view * Nu * Nv;
+    T* __restrict__ dst = out + view * Nu * Nv;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int u = u0 + threadIdx.x, v = v0 + r;
+        if (u < Nu && v < Nv) {
+            T x = src[(size_t)v * Nu + u];
+            if (w) x = T(float(x) * __ldg(w + (size_t)v * Nu + u));
+            tile[r][threadIdx.x] = x;
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int v = v0 + threadIdx.x, u = u0 + r;
+        if (u < Nu && v < Nv) dst[(size_t)u * Nv + v] = tile[threadIdx.x][r];
+    }
 }
 
 // ---- back projection (ray-driven, into a z-slab) ---------------------------------------------
@@ -682,7 +688,7 @@ __global__ void __launch_bounds__(128) hit_rect_kernel(ExactGeom G, const float4
 
 // Tile list of the 32x4 ray blocks inside each plan view's rectangle of rays
 // crossing the box z in [k0, k1).  Synchronous (plan creation).
-static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T)
+static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T, int4** keep_rect = nullptr)
 {
     const unsigned nv = P.nviews;
     T.prefix.assign(nv + 1, 0);
@@ -698,6 +704,10 @@ static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T)
     if (e == cudaSuccess) e = cudaMemcpy(rect.data(), d_rect, nv * sizeof(int4), cudaMemcpyDeviceToHost);
     cudaFree(d_rect);
     if (e != cudaSuccess) return cuda_fail(e, "ray culling");
+    if (keep_rect) {  // the rectangles on the device too
+        RB_CHECK(P.alloc(keep_rect, nv, "ray rectangles"));
+        RB_CUDA(cudaMemcpy(*keep_rect, rect.data(), nv * sizeof(int4), cudaMemcpyHostToDevice));
+    }
     std::vector<uint2> tiles;
     for (unsigned n = 0; n < nv; ++n) {
         T.prefix[n] = (unsigned)tiles.size();
@@ -715,7 +725,7 @@ static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T)
 
 recon_status_t build_exact_culling(Plan& P)
 {
-    RB_CHECK(build_ray_tiles(P, 0, P.eg.Z, P.fp_tiles));
+    RB_CHECK(build_ray_tiles(P, 0, P.eg.Z, P.fp_tiles, &P.d_view_rect));
     P.bp_tiles.clear();
     if (P.bp_gather) return RECON_OK;  // the gather back projector needs no ray blocks
     const int depth = bp_slab_depth(P);
@@ -782,18 +792,50 @@ recon_status_t exact_fp(Plan& P, const float* vol, unsigned first, unsigned coun
     return launch_fp<0, float, float>(P, vol, first, count, nullptr, out, s);
 }
 
+// Views [0, count) of a sinogram [view][v][u] (times w when given) into the
+// detector-column layout.
+// rect: per view from the first, the rectangles of rays crossing the volume
+// (tiles outside them are left as they are), or null for every tile.
+template <class T>
+static recon_status_t to_columns(const Plan& P, const T* in, const float* w, unsigned count, const int4* rect, T* out,
+                                 cudaStream_t s)
+{
+    for (unsigned v0 = 0; v0 < count; v0 += 65535) {
+        const unsigned nv = std::min(count - v0, 65535u);
+        exact::to_columns_kernel<T><<<dim3((P.eg.Nu + 31) / 32, (P.eg.Nv + 31) / 32, nv), dim3(32, 8), 0, s>>>(
+            in + (size_t)v0 * P.npix, w, P.eg.Nu, P.eg.Nv, rect ? rect + v0 : nullptr, out + (size_t)v0 * P.npix);
+        RB_CUDA(cudaGetLastError());
+    }
+    return RECON_OK;
+}
+
+// The plan's ray rectangles from view `first` for `count` views, when those are
+// plan views.
+static const int4* view_rects_from(const Plan& P, unsigned first, unsigned count)
+{
+    return (P.d_view_rect && first + count <= P.nviews) ? P.d_view_rect + first : nullptr;
+}
+
+// The MLEM ratio of views [first, first+count).  For the gather back projector
+// it is written [view][v][u] into the plan's staging buffer and transposed into
+// the detector-column layout.
 recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ratio, cudaStream_t s,
                               unsigned first, unsigned count)
 {
-    const size_t off = (size_t)first * P.npix, roff = (size_t)first * mlem_ratio_view(P);
+    const size_t off = (size_t)first * P.npix;
     using bf = __nv_bfloat16;
     if (P.opt.sino == RECON_SINO_BF16) {
-        if (mlem_ratio_grouped(P)) return launch_fp<3, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
-        return launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, (bf*)ratio + roff, s);
+        bf* r = mlem_ratio_in_columns(P) ? (bf*)P.d_ratio_rm : (bf*)ratio;
+        RB_CHECK((launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, r + off, s)));
+        if (mlem_ratio_in_columns(P))
+            return to_columns<bf>(P, r + off, nullptr, count, view_rects_from(P, first, count), (bf*)ratio + off, s);
+        return RECON_OK;
     }
-    if (mlem_ratio_grouped(P))
-        return launch_fp<3, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + roff, s);
-    return launch_fp<1, float, float>(P, vol, first, count, (const float*)g + off, (float*)ratio + roff, s);
+    float* r = mlem_ratio_in_columns(P) ? (float*)P.d_ratio_rm : (float*)ratio;
+    RB_CHECK((launch_fp<1, float, float>(P, vol, first, count, (const float*)g + off, r + off, s)));
+    if (mlem_ratio_in_columns(P))
+        return to_columns<float>(P, r + off, nullptr, count, view_rects_from(P, first, count), (float*)ratio + off, s);
+    return RECON_OK;
 }
 
 // Number of (ray, voxel) pairs with positive length: the forward walk with
@@ -874,7 +916,11 @@ recon_status_t exact_count(Plan& P, unsigned long long* out)
 
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s)
 {
-    if (voxel_ratio_grouped(P)) return launch_fp<4, float, float>(P, vol, 0u, P.nviews, g, ratio, s);
+    if (voxel_ratio_in_columns(P)) {
+        float* r = (float*)P.d_ratio_rm;
+        RB_CHECK((launch_fp<2, float, float>(P, vol, 0u, P.nviews, g, r, s)));
+        return to_columns<float>(P, r, nullptr, P.nviews, view_rects_from(P, 0, P.nviews), ratio, s);
+    }
     return launch_fp<2, float, float>(P, vol, 0u, P.nviews, g, ratio, s);
 }
 
@@ -1035,42 +1081,35 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
 #undef RB_GATHER_SLOTS
 }
 
-// Scratch for `count` views in the row-group layout (grown on demand).
-static recon_status_t ensure_row_groups(Plan& P, unsigned count)
+// Scratch for `count` views in the detector-column layout (grown on demand).
+static recon_status_t ensure_column_scratch(Plan& P, unsigned count)
 {
-    if (P.rowgroup_views >= count) return RECON_OK;
-    if (P.d_rowgroups) {
-        cudaFree(P.d_rowgroups);
-        P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), (void*)P.d_rowgroups));
-        P.device_bytes -= (size_t)P.rowgroup_views * row_group_view(P) * sizeof(float);
-        P.d_rowgroups = nullptr;
-        P.rowgroup_views = 0;
+    if (P.colsino_views >= count) return RECON_OK;
+    if (P.d_colsino) {
+        cudaFree(P.d_colsino);
+        P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), (void*)P.d_colsino));
+        P.device_bytes -= (size_t)P.colsino_views * P.npix * sizeof(float);
+        P.d_colsino = nullptr;
+        P.colsino_views = 0;
     }
-    RB_CHECK(P.alloc(&P.d_rowgroups, (size_t)count * row_group_view(P), "row-group sinogram"));
-    P.rowgroup_views = count;
+    RB_CHECK(P.alloc(&P.d_colsino, (size_t)count * P.npix, "detector-column sinogram"));
+    P.colsino_views = count;
     return RECON_OK;
 }
 
-// Elements per view in the row-group layout [v/16][u][v%16].
-size_t row_group_view(const Plan& P) { return (size_t)((P.eg.Nv + kRowGroup - 1) / kRowGroup) * kRowGroup * P.eg.Nu; }
-
-// The MLEM ratio is stored in the row-group layout when the gather back
-// projector reads it, else [v][u].
-bool mlem_ratio_grouped(const Plan& P)
+// The MLEM ratio is stored in the detector-column layout [view][u][v] when the
+// gather back projector reads it, else [view][v][u].
+bool mlem_ratio_in_columns(const Plan& P)
 {
     return P.bp_gather && P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_SIDDON;
 }
 
-// The voxel-driven back projector's ratio (no w) is row-grouped too for EXACT
-// plans in GEOMETRIC mode (no detector tilt there), read by its gather kernel.
-bool voxel_ratio_grouped(const Plan& P)
+// The voxel-driven back projector's ratio (no w) is in detector columns too
+// for EXACT plans in GEOMETRIC mode (no detector tilt there), read by its
+// gather kernel.
+bool voxel_ratio_in_columns(const Plan& P)
 {
     return P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_VOXEL && P.opt.voxel_mode == RECON_VOXEL_GEOMETRIC;
-}
-
-size_t mlem_ratio_view(const Plan& P)
-{
-    return (mlem_ratio_grouped(P) || voxel_ratio_grouped(P)) ? row_group_view(P) : P.npix;
 }
 
 recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, unsigned first, unsigned count,
@@ -1084,9 +1123,9 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
     if (count == 0) return launch_fill(f_update ? f_update : vol, 0.0f, P.nvox, s);
     using bf = __nv_bfloat16;
     if (P.bp_gather) {
-        const size_t qv = row_group_view(P);
+        const size_t qv = P.npix;
         if (sens_mode) return launch_gather<false, float>(P, P.d_wq, 0, first, count, vol, nullptr, s);
-        if (sino_is_rw) {  // the MLEM ratio: row-group layout, carries w
+        if (sino_is_rw) {  // the MLEM ratio: detector columns, carries w
             float* out = f_update ? f_update : vol;
             if (bf16) {
                 if (f_update) return launch_gather<true, bf>(P, (const bf*)sino, qv, first, count, out, sens, s);
@@ -1095,17 +1134,10 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
             if (f_update) return launch_gather<true, float>(P, (const float*)sino, qv, first, count, out, sens, s);
             return launch_gather<false, float>(P, (const float*)sino, qv, first, count, out, nullptr, s);
         }
-        // a sinogram [view][v][u]: weighted by w into the row-group scratch first
-        RB_CHECK(ensure_row_groups(P, count));
-        const int nq = (P.eg.Nv + kRowGroup - 1) / kRowGroup;
-        for (unsigned v0 = 0; v0 < count; v0 += 65535) {
-            const unsigned nv = std::min(count - v0, 65535u);
-            exact::to_row_groups_kernel<<<dim3((P.eg.Nu + 127) / 128, nq, nv), 128, 0, s>>>(
-                (const float*)sino + (size_t)v0 * P.npix, P.d_w, P.eg.Nu, P.eg.Nv,
-                reinterpret_cast<float4*>(P.d_rowgroups + (size_t)v0 * qv));
-            RB_CUDA(cudaGetLastError());
-        }
-        return launch_gather<false, float>(P, P.d_rowgroups, qv, first, count, vol, nullptr, s);
+        // a sinogram [view][v][u]: weighted by w into the detector-column scratch first
+        RB_CHECK(ensure_column_scratch(P, count));
+        RB_CHECK(to_columns<float>(P, (const float*)sino, P.d_w, count, nullptr, P.d_colsino, s));
+        return launch_gather<false, float>(P, P.d_colsino, qv, first, count, vol, nullptr, s);
     }
     if (sens_mode) return launch_bp<1, false, float>(P, nullptr, first, count, vol, nullptr, s);
     if (f_update) {

@@ -111,9 +111,9 @@ struct Plan {
     float2* d_cs = nullptr;    // [view] {cos, sin} of the view angle
     ZParam* d_zp = nullptr;    // [v]
     float* d_w = nullptr;      // [v][u] |p2-p1| / R
-    float* d_wq = nullptr;     // the same in the row-group layout [v/16][u][v%16]
-    float* d_rowgroups = nullptr;  // a sinogram in the row-group layout (gather back projector input)
-    unsigned rowgroup_views = 0;   // views d_rowgroups holds
+    float* d_wq = nullptr;     // the same in the detector-column layout [u][v]
+    float* d_colsino = nullptr;  // a sinogram in the detector-column layout (gather back projector input)
+    unsigned colsino_views = 0;   // views d_colsino holds
     bool bp_gather = false;    // Siddon back projection by the column gather (else ray-driven slabs)
     float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y]
     // back projection: fixed-point accumulators of one z-slab, image layout
@@ -124,6 +124,7 @@ struct Plan {
     // ray blocks crossing the volume (forward projection) and each
     // back-projection z-slab; rays outside them contribute nothing
     RayTiles fp_tiles;
+    int4* d_view_rect = nullptr;  // [view] {u_min, u_max, v_min, v_max} of the rays crossing the volume
     std::vector<RayTiles> bp_tiles;
     TexCache tex;  // voxel-driven back projection
     // scratch view slot for arbitrary-angle single-view calls (index nviews)
@@ -136,6 +137,8 @@ struct Plan {
     unsigned osem_subsets = 0;
     bool sens_valid = false;
     void* d_ratio = nullptr;      // ratio sinogram (float or bf16) [nviews][npix]
+    void* d_ratio_rm = nullptr;   // EXACT gather plans: the ratio as the forward projector writes it,
+                                  // [view][v][u], before its transpose into d_ratio
     float* d_ht = nullptr;        // COMPAT: Ht accumulator [nvox]
     unsigned long long* d_fix = nullptr;  // COMPAT: fixed-point accumulator [nvox]
     unsigned* d_maxabs = nullptr; // COMPAT: per-view max |value| bits [nviews+1]
@@ -194,7 +197,7 @@ recon_status_t compat_sensitivity(Plan& P, float* sens, cudaStream_t s);
 
 recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned count, bool scratch_slot,
                         float angle_scratch, unsigned Nproj, int mode, bool ones, float* vol_accum,
-                        const float* sens, float* f_update, cudaStream_t s, bool rowgrouped = false);
+                        const float* sens, float* f_update, cudaStream_t s, bool columns = false);
 recon_status_t plain_fp_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
 recon_status_t compat_fp_ratio_all(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s);
@@ -209,14 +212,11 @@ int bp_slab_depth(const Plan& P);
 bool exact_bp_gather_suits(const Plan& P);
 recon_status_t march_fp_view(Plan& P, const float* vol, float angle_deg, int mode, float* img, cudaStream_t s);
 int exact_bp_gather_max_rows();
-size_t mlem_ratio_view(const Plan& P);
-bool voxel_ratio_grouped(const Plan& P);
+bool voxel_ratio_in_columns(const Plan& P);
 int gather_slots(int Z);
-// Row-group layout of sinograms read by the gather back projector:
-// [view][v / kRowGroup][u][v % kRowGroup].
-constexpr int kRowGroup = 16, kRowGroupShift = 4;
-size_t row_group_view(const Plan& P);
-bool mlem_ratio_grouped(const Plan& P);
+// Sinograms read by the gather back projectors are in the detector-column
+// layout [view][u][v].
+bool mlem_ratio_in_columns(const Plan& P);
 recon_status_t build_exact_culling(Plan& P);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);

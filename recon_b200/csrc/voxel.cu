@@ -235,9 +235,9 @@ __global__ void __launch_bounds__(128) bp_column_kernel(VGeom G, const float* __
 // bottom voxel centre vA (with the row step per voxel vB) are set up 32 views
 // at a time, one per lane, in shared memory; then every lane samples its
 // voxels' rows v = vA + k vB with the same bilinear arithmetic as
-// bp_column_kernel.  The view images are read in the row-group layout
-// [view][v/16][u][v%16] (view_stride elements per view), so one tap of all 32
-// lanes (about 26 consecutive rows of one detector column) lies in one or two
+// bp_column_kernel.  The view images are read in the detector-column layout
+// [view][u][v] (view_stride elements per view), so one tap of all 32 lanes
+// (about 26 consecutive rows of one detector column) lies in one or two
 // 128-byte lines.  The taps of four voxels are loaded before any is used.  MODE
 // as in bp_kernel; MODE 1 reads nothing.
 constexpr int kVoxelWarps = 8;  // a 4 x 2 tile of columns per CTA
@@ -261,7 +261,6 @@ __global__ void __launch_bounds__(kVoxelWarps * 32, 3) bp_gather_kernel(VGeom G,
     const float cu = (float)(G.Nu - 1) * 0.5f, cv = (float)(G.Nv - 1) * 0.5f;
     const float umax = (float)(G.Nu - 1), vmax = (float)(G.Nv - 1);
     const float inv_n = 1.0f / (float)Nproj;
-    const int grow = kRowGroup * G.Nu - kRowGroup;  // row v of a detector column: v + (v / kRowGroup) * grow
     for (int k0 = 0; k0 < G.Z; k0 += 32 * SLOTS) {
         const float z0 = center((float)G.Z, G.vox[2], 1.0f, k0);
         float acc[SLOTS];
@@ -288,7 +287,7 @@ __global__ void __launch_bounds__(kVoxelWarps * 32, 3) bp_gather_kernel(VGeom G,
                 if (!(u_pix >= 0.0f && u_pix <= umax)) continue;
                 const int ui = min(max((int)floorf(u_pix), 0), G.Nu - 2);
                 const float uw = u_pix - (float)ui;
-                const float* __restrict__ col = rg + (size_t)(vb + q) * view_stride + (size_t)ui * kRowGroup;
+                const float* __restrict__ col = rg + (size_t)(vb + q) * view_stride + (size_t)ui * G.Nv;
                 const float vbase = fmaf((float)lane, V.z, V.y);
                 // taps of PH voxels at a time, loaded before any is used: rows are
                 // clamped to the image, so every address is valid, and voxels whose
@@ -308,12 +307,11 @@ __global__ void __launch_bounds__(kVoxelWarps * 32, 3) bp_gather_kernel(VGeom G,
                         const int vj = (int)min(__float2uint_rd(v_pix), (unsigned)G.Nv - 2u);
                         vw[jj] = v_pix - (float)vj;
                         if (MODE != 1) {
-                            const float* r0 = col + vj + (vj >> kRowGroupShift) * grow;
-                            const float* r1 = col + (vj + 1) + ((vj + 1) >> kRowGroupShift) * grow;
+                            const float* r0 = col + vj;
                             t00[jj] = __ldg(r0);
-                            t10[jj] = __ldg(r0 + kRowGroup);
-                            t01[jj] = __ldg(r1);
-                            t11[jj] = __ldg(r1 + kRowGroup);
+                            t10[jj] = __ldg(r0 + G.Nv);
+                            t01[jj] = __ldg(r0 + 1);
+                            t11[jj] = __ldg(r0 + 1 + G.Nv);
                         }
                     }
 #pragma unroll
@@ -423,12 +421,12 @@ static void release_textures(TexCache& c)
 
 void release_plan_textures(Plan* P) { release_textures(P->tex); }
 
-// rowgrouped: sino is in the row-group layout (the MLEM ratio of an EXACT
-// plan with this back projector), else [view][v][u].
+// columns: sino is in the detector-column layout [view][u][v] (the MLEM ratio
+// of an EXACT plan with this back projector), else [view][v][u].
 template <int VMODE, int MODE>
 static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angles, unsigned first, unsigned count,
                                    unsigned Nproj, float* vol, const float* sens, bool cache_textures,
-                                   bool rowgrouped, cudaStream_t s)
+                                   bool columns, cudaStream_t s)
 {
     voxel::VGeom G = vgeom(P);
     dim3 blk(32, 4, 1), grid((G.X + 31) / 32, (G.Y + 3) / 4, G.Z);
@@ -436,7 +434,7 @@ static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angl
     cudaTextureObject_t* d_handles = nullptr;
     std::vector<cudaTextureObject_t> local;
     cudaTextureObject_t* d_local = nullptr;
-    if (VMODE == RECON_VOXEL_GEOMETRIC && MODE != 1 && sino && !rowgrouped) {
+    if (VMODE == RECON_VOXEL_GEOMETRIC && MODE != 1 && sino && !columns) {
         if (cache_textures) {
             TexCache& c = P.tex;
             if (c.base != sino || c.count != count) {
@@ -462,9 +460,9 @@ static recon_status_t launch_voxel(Plan& P, const float* sino, const float* angl
         }
     }
     const bool untilted = P.geom.cal.xangle == 0.0f && P.geom.cal.yangle == 0.0f && P.geom.cal.zangle == 0.0f;
-    if (VMODE == RECON_VOXEL_GEOMETRIC && untilted && (MODE == 1 || rowgrouped)) {
+    if (VMODE == RECON_VOXEL_GEOMETRIC && untilted && (MODE == 1 || columns)) {
         const dim3 ggrid((G.X + 3) / 4, (G.Y + 1) / 2);
-        const size_t stride = row_group_view(P);
+        const size_t stride = P.npix;
         switch (gather_slots(G.Z)) {
 #define RB_VOXEL_SLOTS(n)                                                                                          \
     case n:                                                                                                        \
@@ -515,7 +513,7 @@ __global__ void voxel_set_angle_kernel(float* p, float v) { *p = v; }
 
 recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned count, bool scratch_slot,
                         float angle_scratch, unsigned Nproj, int mode, bool ones, float* vol_accum,
-                        const float* sens, float* f_update, cudaStream_t s, bool rowgrouped)
+                        const float* sens, float* f_update, cudaStream_t s, bool columns)
 {
     if (scratch_slot) {
         voxel_set_angle_kernel<<<1, 1, 0, s>>>(P.d_angles + P.nviews, angle_scratch);
@@ -532,14 +530,14 @@ recon_status_t voxel_bp(Plan& P, const float* sino, unsigned first, unsigned cou
     }
     if (f_update) {
         return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 2>(P, sino, P.d_angles, first, count, Nproj, f_update, sens,
-                                                             cache, rowgrouped, s)
+                                                             cache, columns, s)
                    : launch_voxel<RECON_VOXEL_GEOMETRIC, 2>(P, sino, P.d_angles, first, count, Nproj, f_update, sens,
-                                                             cache, rowgrouped, s);
+                                                             cache, columns, s);
     }
     return ref ? launch_voxel<RECON_VOXEL_REFERENCE, 0>(P, sino, P.d_angles, first, count, Nproj, vol_accum, nullptr,
-                                                         cache, rowgrouped, s)
+                                                         cache, columns, s)
                : launch_voxel<RECON_VOXEL_GEOMETRIC, 0>(P, sino, P.d_angles, first, count, Nproj, vol_accum, nullptr,
-                                                         cache, rowgrouped, s);
+                                                         cache, columns, s);
 }
 
 }  // namespace rb
