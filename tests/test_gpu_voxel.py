@@ -81,7 +81,7 @@ def test_mlem_with_voxel_bp_converges():
 @pytest.mark.parametrize("zdim", [40, 300])
 def test_mlem_iteration_matches_per_view_path(zdim):
     # an EXACT plan's MLEM iteration with the voxel-driven back projector (the
-    # ratio in the row-group layout, read by the column gather kernel) against the
+    # ratio in the detector-column layout, read by the column gather kernel) against the
     # same iteration assembled from the forward projector and single-view voxel
     # back projections of row-major images (the texture kernels)
     cfg = small_cfg(Zdim=zdim, ZVoxSize=0.2 if zdim > 100 else 1.0, NumProj=10)
