@@ -236,11 +236,14 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
         // when that is the same count for every lane, else -1.  The bound f0 of voxel k
         // is min over the piece of z_k * c and f1 the max of z_k+1 * c: c = ez / (depth)
         // is larger at the piece's near end, so the near end gives f0 below z = 0 and
-        // f1 above, the far end the others.  Rounding can make the other end's value
-        // pass by an ulp, which moves a bound only where it lies a row's 0.002 margin
-        // away from the voxel: the row it adds or drops has no length there.
-        const int rel = (G.Z + 1) / 2 - k0;
-        const int split = rel <= 0 ? 0 : (rel >= 32 * SLOTS ? SLOTS : (rel % 32 == 0 ? rel / 32 : -1));
+        // f1 above, the far end the others.  Z must be even: for odd Z the middle voxel
+        // straddles z = 0 (its bottom below, its top above).  Rounding can make the
+        // other end's value pass by an ulp, which moves a bound only where it lies a
+        // row's 0.002 margin away from the voxel: the row it adds or drops has no
+        // length there.
+        const int rel = G.Z / 2 - k0;
+        const int split = (G.Z & 1) ? -1
+                          : rel <= 0 ? 0 : (rel >= 32 * SLOTS ? SLOTS : (rel % 32 == 0 ? rel / 32 : -1));
         const float fk0 = (float)(k0 + lane);
         const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
         const int nslot = min(SLOTS, max(0, (G.Z - k0 - lane + 31) / 32));

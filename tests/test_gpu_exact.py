@@ -280,6 +280,19 @@ def test_mlem_iteration_designs_agree(name):
     assert ((fs[0] - fs[1]).norm() / fs[1].norm()).item() < 1e-5
 
 
+def test_odd_height_gather_vs_fp64():
+    # 255 slices in one chunk of 8 voxels per lane: the middle voxel straddles the
+    # source plane, so the gather takes both ends of each piece for its row bounds
+    cfg = small_cfg(Xdim=16, Ydim=16, Zdim=255, ZVoxSize=0.25, TAxPixDim=0.5, TAxPixels=160, NumProj=6)
+    P = Plan(cfg, Options(siddon_bp=SIDDON_BP_GATHER))
+    g = O.Geom.from_dict(geom_dict(cfg))
+    nproj = int(cfg["NumProj"])
+    sino = np.random.default_rng(13).random(nproj * g.npix).astype(np.float32)
+    ref = O.x_bp_all(g, nproj, np.float32(cfg["DeltaAng"]), sino.astype(np.float64))
+    out = P.bp_views(torch.from_numpy(sino).cuda().reshape(nproj, P.nv, P.nu)).cpu().numpy().ravel()
+    assert rel_l2(out, ref) < 1e-5, rel_l2(out, ref)
+
+
 # A tall, thin volume: the gather works through the column in five z-chunks of 224 slices.
 TALL = small_cfg(Xdim=4, Ydim=4, Zdim=1100, XVoxSize=0.05, YVoxSize=0.05, ZVoxSize=0.05, AxPixels=8,
                  TAxPixels=900, AxPixDim=0.1, TAxPixDim=0.1, NumProj=4)
