@@ -294,6 +294,17 @@ recon_status_t recon_batch_mlem(recon_batch_t batch, const float* const* d_g, fl
  * NumProj views (EXACT arithmetic): the I of the throughput figure
  * "ray-voxel intersections per second".  Synchronous. */
 recon_status_t recon_count_intersections(recon_plan_t plan, unsigned long long* count);
+/* The same count as one projector of the plan produces it: the (ray, voxel)
+ * pairs that the forward projector (projector = RECON_PROJECTOR_FORWARD) or
+ * the Siddon back projector (RECON_PROJECTOR_BACK) gives a positive length.
+ * Equal to recon_count_intersections when no projector drops or adds a pair;
+ * where a projector is the ray walk itself (the ray-driven back projector, or
+ * the forward walk where the detector-column forward projector does not
+ * apply) it is that count.  EXACT arithmetic, synchronous.  A parity check
+ * with no counterpart in the reference. */
+#define RECON_PROJECTOR_FORWARD 0
+#define RECON_PROJECTOR_BACK 1
+recon_status_t recon_count_projector_pairs(recon_plan_t plan, int projector, unsigned long long* count);
 
 /* ---- elementwise drop-ins (hf_cuda_kernels.cuh) -------------------------- */
 

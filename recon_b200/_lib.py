@@ -25,6 +25,8 @@ BP_SIDDON, BP_VOXEL = 0, 1
 VOXEL_REFERENCE, VOXEL_GEOMETRIC = 0, 1
 SIDDON_BP_AUTO, SIDDON_BP_GATHER, SIDDON_BP_RAY = 0, 1, 2
 NOALLOC_MAX_VOXELS = 2097152  # RECON_NOALLOC_MAX_VOXELS
+PROJECTOR_FORWARD = 0  # RECON_PROJECTOR_FORWARD
+PROJECTOR_BACK = 1  # RECON_PROJECTOR_BACK
 ABI_VERSION = 2  # RECON_B200_ABI_VERSION: the layout of the structures above
 
 
@@ -113,6 +115,7 @@ def lib() -> C.CDLL:
         "recon_mlem_update": (st, [P, P, P, P]),
         "recon_mlem_backward_update": (st, [P, P, P]),
         "recon_count_intersections": (st, [P, C.POINTER(C.c_ulonglong)]),
+        "recon_count_projector_pairs": (st, [P, C.c_int, C.POINTER(C.c_ulonglong)]),
         "recon_view_step_count": (st, [P, f, up]),
         "recon_set_ones": (st, [P, C.c_size_t, P]),
         "recon_divide1": (st, [P, P, C.c_size_t, P]),
@@ -145,7 +148,7 @@ def exported_symbols() -> list[str]:
         "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_fp_view", "recon_fp_views",
         "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_march_fp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
-        "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_set_ones", "recon_divide1", "recon_multiply1",
+        "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_count_projector_pairs", "recon_set_ones", "recon_divide1", "recon_multiply1",
         "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_view_step_count", "recon_mlem_from_cfg",
         "recon_forward_projection_from_cfg", "recon_backward_projection_from_cfg", "recon_batch_create",
         "recon_batch_destroy", "recon_batch_mlem", "recon_compat_bp_view_noalloc", "recon_osem",

@@ -223,6 +223,13 @@ class Plan:
         check(lib().recon_count_intersections(self._h, C.byref(n)))
         return int(n.value)
 
+    def count_projector_pairs(self, projector: int) -> int:
+        """(ray, voxel) pairs of positive length as PROJECTOR_FORWARD or
+        PROJECTOR_BACK assigns them (recon_count_projector_pairs)."""
+        n = C.c_ulonglong()
+        check(lib().recon_count_projector_pairs(self._h, int(projector), C.byref(n)))
+        return int(n.value)
+
     # --- parity (COMPAT) ---
     def compat_setup_view(self, angle: float) -> tuple[int, dict]:
         n = self.nu * self.nv

@@ -189,7 +189,7 @@ recon_status_t ensure_mlem_buffers(Plan& P)
         // zero outside the ray blocks the forward projector writes (EXACT culling)
         RB_CUDA(cudaMemset(q, 0, n * es));
         P.d_ratio = q;
-        if (P.opt.arith == RECON_ARITH_EXACT && (mlem_ratio_in_columns(P) || voxel_ratio_in_columns(P))) {
+        if (P.opt.arith == RECON_ARITH_EXACT && !P.fp_column && (mlem_ratio_in_columns(P) || voxel_ratio_in_columns(P))) {
             RB_CHECK(P.alloc(&q, n * es, "ratio sinogram (staging)"));
             RB_CUDA(cudaMemset(q, 0, n * es));
             P.d_ratio_rm = q;
@@ -283,7 +283,14 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CUDA(cudaMemset(P->d_wq, 0, P->npix * sizeof(float)));
             if (P->bp_gather && P->eg.Nv > exact_bp_gather_max_rows())
                 return fail(RECON_ERR_UNSUPPORTED, "the gather back projector takes at most 12288 detector rows");
-            RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
+            P->fp_column = exact_fp_column_suits(*P);
+            if (P->fp_column) {
+                const size_t nz = (size_t)P->eg.X * P->eg.Y * (P->eg.Z + 2);
+                RB_CHECK(P->alloc(&P->d_vol_z, nz, "z-fastest volume"));
+                RB_CUDA(cudaMemset(P->d_vol_z, 0, nz * sizeof(float)));  // the zero layers stay zero
+            } else {
+                RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
+            }
             if (!P->bp_gather) {  // the ray-driven back projector's slab accumulators
                 const size_t slab = (size_t)P->eg.X * P->eg.Y * bp_slab_depth(*P);
                 RB_CHECK(P->alloc(&P->d_bpacc, slab, "back projection accumulator"));
@@ -555,6 +562,18 @@ recon_status_t recon_count_intersections(recon_plan_t P, unsigned long long* cou
     if (P->opt.arith != RECON_ARITH_EXACT) return fail(RECON_ERR_UNSUPPORTED, "counting uses EXACT arithmetic");
     RB_CHECK(use_device(*P));
     return exact_count(*P, count);
+}
+
+recon_status_t recon_count_projector_pairs(recon_plan_t P, int projector, unsigned long long* count)
+{
+    if (!P || !count) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (P->opt.arith != RECON_ARITH_EXACT) return fail(RECON_ERR_UNSUPPORTED, "counting uses EXACT arithmetic");
+    if (projector != RECON_PROJECTOR_FORWARD && projector != RECON_PROJECTOR_BACK)
+        return fail(RECON_ERR_INVALID_ARGUMENT, "projector must be RECON_PROJECTOR_FORWARD or RECON_PROJECTOR_BACK");
+    RB_CHECK(use_device(*P));
+    if (projector == RECON_PROJECTOR_FORWARD && P->fp_column) return exact_fp_column_count(*P, count);
+    if (projector == RECON_PROJECTOR_BACK && P->bp_gather) return exact_bp_gather_count(*P, count);
+    return exact_count(*P, count);  // the ray walk, which these projectors run
 }
 
 recon_status_t recon_mlem(recon_plan_t P, const void* d_g, unsigned iters, float* d_f, int init_ones, void* stream)

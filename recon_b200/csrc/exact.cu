@@ -179,8 +179,10 @@ __global__ void __launch_bounds__(128, 10) fp_kernel(ExactGeom G, const float4* 
 // Values are read in the detector-column layout [view][u][v] (view_stride
 // elements per view; 0 for the weights w of the sensitivity): a warp's loads of
 // nearby rows of one detector column fall in one or two 128-byte lines, and a
-// row's element is one add from its column.  UPDATE:
-// f = (sens != 0) ? f * Ht / sens : 0; otherwise vol = Ht.
+// row's element is one add from its column.  EPI 1 (MLEM update):
+// f = (sens != 0) ? f * Ht / sens : 0; EPI 0: vol = Ht; EPI 2: no image, the
+// number of (ray, voxel) pairs given a positive length is added to *npairs
+// (a check that the candidate margins drop no pair of the forward walk).
 constexpr int kGatherWarps = 8;  // a kGatherTileX x (8 / kGatherTileX) tile of columns per CTA
 constexpr int kGatherTileX = 4;
 // SLOTS: voxels per lane and chunk (chunks of 32 * SLOTS slices; 8 unless the
@@ -200,11 +202,12 @@ struct GatherView {
     unsigned single;  // bit sl: no voxel of the column has a second candidate row at u_lo + sl
 };
 
-template <bool UPDATE, class ST, int SLOTS>
+template <int EPI, class ST, int SLOTS>
 __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
     const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned view0, unsigned nview,
-    const ST* __restrict__ vals, size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens)
+    const ST* __restrict__ vals, size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens,
+    unsigned long long* __restrict__ npairs)
 {
     // row v's z planes: voxel k spans t in [fmaf(k - z, S, O), fmaf(k - w, S, O)]
     // with {S, O, z, w} = szq[v] (z = kc, w = kc - 1 when S > 0; swapped when S < 0)
@@ -332,7 +335,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                             const float t = fk0 + (float)(32 * s);
                             const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
                             const float L = fminf(B, hi) - fmaxf(A, lo);
-                            if (L > 0.0f) acc[s] = fmaf(L, x, acc[s]);
+                            if (L > 0.0f) acc[s] = (EPI == 2) ? acc[s] + 1.0f : fmaf(L, x, acc[s]);
                         };
                         if (!(A + G.Rf > 1e-3f * G.Rf)) {  // a piece behind the source: every row is a candidate
 #pragma unroll
@@ -409,7 +412,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                                     const float4 zr = szq[v];
                                     const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
                                     const float L = fminf(B, hi) - fmaxf(A, lo);
-                                    if (L > 0.0f) sum = fmaf(L, load_val<ST>(col + v), sum);
+                                    if (L > 0.0f) sum = (EPI == 2) ? sum + 1.0f : fmaf(L, load_val<ST>(col + v), sum);
                                 }
                                 acc2[s * 32 + lane] = sum;
                             }
@@ -419,12 +422,21 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                 __syncwarp();  // the next batch rewrites sv
             }
         }
+        if (EPI == 2) {  // pair counts (exact: a voxel's count stays far below 2^24)
+            unsigned long long c = 0;
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s)
+                if (s < nslot) c += (unsigned long long)(acc[s] + acc2[s * 32 + lane]);
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0 && c) atomicAdd(npairs, c);
+            continue;
+        }
 #pragma unroll
         for (int s = 0; s < SLOTS; ++s) {
             if (s >= nslot) continue;
             const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)(k0 + lane + 32 * s) * plane;
             const float ht = acc[s] + acc2[s * 32 + lane];
-            if (UPDATE) {
+            if (EPI == 1) {
                 const float svv = sens[vox];
                 vol[vox] = (svv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[vox], ht), svv) : 0.0f;
             } else {
@@ -691,7 +703,8 @@ __global__ void __launch_bounds__(128) hit_rect_kernel(ExactGeom G, const float4
 
 // Tile list of the 32x4 ray blocks inside each plan view's rectangle of rays
 // crossing the box z in [k0, k1).  Synchronous (plan creation).
-static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T, int4** keep_rect = nullptr)
+static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T, int4** keep_rect = nullptr,
+                                      std::vector<int4>* host_rect = nullptr)
 {
     const unsigned nv = P.nviews;
     T.prefix.assign(nv + 1, 0);
@@ -707,6 +720,7 @@ static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T, int4
     if (e == cudaSuccess) e = cudaMemcpy(rect.data(), d_rect, nv * sizeof(int4), cudaMemcpyDeviceToHost);
     cudaFree(d_rect);
     if (e != cudaSuccess) return cuda_fail(e, "ray culling");
+    if (host_rect) *host_rect = rect;
     if (keep_rect) {  // the rectangles on the device too
         RB_CHECK(P.alloc(keep_rect, nv, "ray rectangles"));
         RB_CUDA(cudaMemcpy(*keep_rect, rect.data(), nv * sizeof(int4), cudaMemcpyHostToDevice));
@@ -728,7 +742,9 @@ static recon_status_t build_ray_tiles(Plan& P, int k0, int k1, RayTiles& T, int4
 
 recon_status_t build_exact_culling(Plan& P)
 {
-    RB_CHECK(build_ray_tiles(P, 0, P.eg.Z, P.fp_tiles, &P.d_view_rect));
+    std::vector<int4> rect;
+    RB_CHECK(build_ray_tiles(P, 0, P.eg.Z, P.fp_tiles, &P.d_view_rect, &rect));
+    if (P.fp_column && P.nviews) RB_CHECK(build_column_tiles(P, rect));
     P.bp_tiles.clear();
     if (P.bp_gather) return RECON_OK;  // the gather back projector needs no ray blocks
     const int depth = bp_slab_depth(P);
@@ -792,6 +808,7 @@ recon_status_t exact_fp(Plan& P, const float* vol, unsigned first, unsigned coun
         first = P.nviews;
         count = 1;
     }
+    if (P.fp_column) return exact_fp_column(P, vol, first, count, out, s);
     return launch_fp<0, float, float>(P, vol, first, count, nullptr, out, s);
 }
 
@@ -827,6 +844,12 @@ recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ra
 {
     const size_t off = (size_t)first * P.npix;
     using bf = __nv_bfloat16;
+    if (P.fp_column) {  // straight into the layout the back projector reads
+        const bool bf16 = P.opt.sino == RECON_SINO_BF16;
+        const size_t es = bf16 ? sizeof(bf) : sizeof(float);
+        return exact_fp_column_ratio(P, vol, (const char*)g + off * es, (char*)ratio + off * es, 1,
+                                     mlem_ratio_in_columns(P), bf16, first, count, s);
+    }
     if (P.opt.sino == RECON_SINO_BF16) {
         bf* r = mlem_ratio_in_columns(P) ? (bf*)P.d_ratio_rm : (bf*)ratio;
         RB_CHECK((launch_fp<1, bf, bf>(P, vol, first, count, (const bf*)g + off, r + off, s)));
@@ -919,6 +942,7 @@ recon_status_t exact_count(Plan& P, unsigned long long* out)
 
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s)
 {
+    if (P.fp_column) return exact_fp_column_ratio(P, vol, g, ratio, 2, voxel_ratio_in_columns(P), false, 0u, P.nviews, s);
     if (voxel_ratio_in_columns(P)) {
         float* r = (float*)P.d_ratio_rm;
         RB_CHECK((launch_fp<2, float, float>(P, vol, 0u, P.nviews, g, r, s)));
@@ -1032,9 +1056,10 @@ bool exact_bp_gather_suits(const Plan& P)
 // arrays, within the 227 KB a block may use.
 int exact_bp_gather_max_rows() { return 12288; }
 
-template <bool UPDATE, class ST, int SLOTS>
+template <int EPI, class ST, int SLOTS>
 static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_stride, unsigned first,
-                                          unsigned count, float* vol, const float* sens, cudaStream_t s)
+                                          unsigned count, float* vol, const float* sens, cudaStream_t s,
+                                          unsigned long long* npairs = nullptr)
 {
     const ExactGeom& E = P.eg;
     exact::GatherConst C;
@@ -1043,7 +1068,7 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
     C.ez = (float)((double)E.Ry / E.dv);
     C.oz = (float)(-((double)E.Dz + E.vd0) / E.dv);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
-    auto kernel = exact::bp_gather_kernel<UPDATE, ST, SLOTS>;
+    auto kernel = exact::bp_gather_kernel<EPI, ST, SLOTS>;
     const size_t static_smem = sizeof(exact::GatherView) * 32 * exact::kGatherWarps +  // sview
                                sizeof(float) * exact::kGatherWarps * SLOTS * 32;         // sacc2
     if (smem + static_smem > 48 * 1024)
@@ -1051,7 +1076,7 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
     constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
     const dim3 grid((E.X + tx - 1) / tx, (E.Y + ty - 1) / ty);
     kernel<<<grid, exact::kGatherWarps * 32, smem, s>>>(E, C, P.d_txy, P.d_kxy, P.d_cs, P.d_zp, first, count, vals,
-                                                         view_stride, vol, sens);
+                                                         view_stride, vol, sens, npairs);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
@@ -1065,12 +1090,13 @@ int gather_slots(int Z)
     return std::min(8, std::max(1, (Z + 32 * chunks - 1) / (32 * chunks)));
 }
 
-template <bool UPDATE, class ST>
+template <int EPI, class ST>
 static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride, unsigned first, unsigned count,
-                                    float* vol, const float* sens, cudaStream_t s)
+                                    float* vol, const float* sens, cudaStream_t s,
+                                    unsigned long long* npairs = nullptr)
 {
 #define RB_GATHER_SLOTS(n) \
-    case n: return launch_gather_slots<UPDATE, ST, n>(P, vals, view_stride, first, count, vol, sens, s)
+    case n: return launch_gather_slots<EPI, ST, n>(P, vals, view_stride, first, count, vol, sens, s, npairs)
     switch (gather_slots(P.eg.Z)) {
         RB_GATHER_SLOTS(1);
         RB_GATHER_SLOTS(2);
@@ -1079,9 +1105,28 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
         RB_GATHER_SLOTS(5);
         RB_GATHER_SLOTS(6);
         RB_GATHER_SLOTS(7);
-        default: return launch_gather_slots<UPDATE, ST, 8>(P, vals, view_stride, first, count, vol, sens, s);
+        default: return launch_gather_slots<EPI, ST, 8>(P, vals, view_stride, first, count, vol, sens, s, npairs);
     }
 #undef RB_GATHER_SLOTS
+}
+
+// (ray, voxel) pairs the gather back projector gives a positive length, over
+// all plan views (synchronous).  Its candidate rows and detector columns are
+// found with margins; this count equals the forward walk's exactly when no
+// pair is lost to them.
+recon_status_t exact_bp_gather_count(Plan& P, unsigned long long* total)
+{
+    unsigned long long* d = nullptr;
+    RB_CUDA(cudaMalloc(&d, sizeof(unsigned long long)));
+    cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
+    recon_status_t st = RECON_OK;
+    if (e == cudaSuccess && P.nviews)
+        st = launch_gather<2, float>(P, P.d_wq, 0, 0u, P.nviews, nullptr, nullptr, 0, d);
+    if (e == cudaSuccess && st == RECON_OK) e = cudaMemcpy(total, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (st != RECON_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "gather pair count");
+    return RECON_OK;
 }
 
 // Scratch for `count` views in the detector-column layout (grown on demand).

@@ -1,0 +1,452 @@
+// fpcol.cu -- EXACT forward projection by detector columns.
+//
+// With no detector tilt, every ray of one detector column (view, u) crosses the
+// same (x, y) voxel columns at the same t: its x and y plane crossings depend on
+// (view, u) only, its z crossings on the row v only.  A CTA therefore builds the
+// column's xy path once -- piece j is the rays' stretch [t_{j-1}, t_j] inside one
+// (x, y) voxel column, found by ranking every x crossing among the y crossings
+// and the other way round (a thread-parallel merge, ties x first as in the ray
+// walk) -- and each warp walks the path for 32 consecutive detector rows, one
+// row per lane.  A lane tracks only its row's z planes: per piece it adds
+//     (m - t_{j-1}) * f[layer] + (t_j - m) * f[next layer],   m = min(t_z, t_j),
+// and steps to the next layer when its next z plane t_z falls inside the piece.
+// The plan uses this kernel only where a piece spans less than a voxel of z
+// (0.9 at most, from the steepest row and the column diagonal), so a piece
+// holds at most one z crossing.  The volume is read from a z-fastest copy with
+// a zero layer below and above every column: the 32 rows of a warp read
+// neighbouring addresses, and a row outside the volume reads zeros, which
+// spares the lanes any entry and exit tests except where a row leaves the
+// volume through its top or bottom before the path ends.
+//
+// Every (ray, voxel) pair gets the length min(t_j, hi_z) - max(t_{j-1}, lo_z)
+// from the plane values plane_t of the ray walk (exact_device.cuh) and of both
+// back projectors, so the projector pair stays an exact transpose; only the
+// order of the ray sum's additions differs from the walk.  Ray sums are
+// compensated (Kahan) over blocks of 8 pieces: each block's 16 products are
+// summed in FP32 and the block sums Kahan-added.
+#include "exact_device.cuh"
+#include "internal.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+
+namespace rb {
+namespace exact {
+
+constexpr int kColWarps = 4;               // warps per CTA, 32 detector rows each
+constexpr int kColRows = 32 * kColWarps;   // rows per CTA
+
+// Number of b in [0, n) whose plane value fmaf(q0 + b*d, S, O) lies before t
+// (strictly when LT, else at or before); the values increase with b (d has the
+// sign of S).  Estimated from the first value and the step |S|, then corrected
+// against the FP32 plane values themselves.
+template <bool LT>
+__device__ __forceinline__ int count_before(float t, int q0, int d, float S, float O, float inv_abs_S, int n)
+{
+    auto before = [&](int b) {
+        const float tb = fmaf((float)(q0 + b * d), S, O);
+        return LT ? (tb < t) : (tb <= t);
+    };
+    int c = (int)ceilf((t - fmaf((float)q0, S, O)) * inv_abs_S);
+    c = min(max(c, 0), n);
+    while (c < n && before(c)) ++c;
+    while (c > 0 && !before(c - 1)) --c;
+    return c;
+}
+
+// Smallest piece index j in [0, n) whose end spc[j].x is after t (STRICT) or at
+// or after t; the last piece ends at the path's exit, which the callers' t
+// never passes.
+template <bool STRICT>
+__device__ __forceinline__ int first_piece_ending(const float2* spc, int n, float t)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const float e = spc[mid].x;
+        if (STRICT ? (e > t) : (e >= t)) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void kahan_add(float& acc, float& comp, float x)
+{
+    const float y = x - comp;
+    const float t = acc + y;
+    comp = (t - acc) - y;
+    acc = t;
+}
+
+// One warp's rows over pieces jb..je.  Per lane: cur = start of the next
+// piece, kaddr = offset of the row's current layer in a padded column (layer
+// k at k + 1), kf = index of the next z plane minus kc as a float, tzn = that
+// plane's t.  STEP = the layer step of every lane (+1 or -1), or 0 for a
+// warp with rows of both directions (step then holds each lane's).  Unless
+// FAST, a lane that leaves through the far face (kaddr reaching kexit) parks
+// its next plane at infinity.  COUNT: no volume reads; the result is the
+// number of pieces of positive length the row has inside the volume (its
+// (ray, voxel) pairs).
+template <bool KAHAN, bool FAST, int STEP, bool COUNT>
+__device__ __forceinline__ float walk_rows(const float* __restrict__ volz, const float2* spc, int jb, int je, float cur,
+                                           int kaddr, float kf, float tzn, float S, float O, int step, int kexit,
+                                           int Z)
+{
+    const int st = STEP != 0 ? STEP : step;
+    const float fst = (float)st;
+    float acc = 0.0f, comp = 0.0f, f1 = 0.0f;
+    auto piece = [&](int j, float& blk) {
+        const float2 pc = spc[j];
+        const float B = pc.x;
+        const float* p = volz + (__float_as_int(pc.y) + kaddr);
+        const bool cross = tzn < B;
+        const float m = fminf(tzn, B);
+        if (COUNT) {  // layers 0 .. Z-1 sit at kaddr 1 .. Z
+            blk += (m - cur > 0.0f && (unsigned)(kaddr - 1) < (unsigned)Z) ? 1.0f : 0.0f;
+            blk += (B - m > 0.0f && (unsigned)(kaddr + st - 1) < (unsigned)Z) ? 1.0f : 0.0f;
+        } else {
+            const float f0 = __ldg(p);
+            if (cross) f1 = __ldg(p + st);
+            blk = fmaf(m - cur, f0, blk);
+            blk = fmaf(B - m, f1, blk);  // B - m = 0 without a crossing
+        }
+        if (cross) {
+            kaddr += st;
+            kf += fst;
+            tzn = fmaf(kf, S, O);
+            if (!FAST && kaddr == kexit) tzn = __int_as_float(0x7f800000);
+        }
+        cur = B;
+    };
+    int j = jb;
+    for (; j + 7 <= je; j += 8) {
+        float blk = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) piece(j + q, blk);
+        if (KAHAN && !COUNT) kahan_add(acc, comp, blk);
+        else acc += blk;
+    }
+    float blk = 0.0f;
+#pragma unroll 1
+    for (; j <= je; ++j) piece(j, blk);
+    if (KAHAN && !COUNT) {
+        kahan_add(acc, comp, blk);
+        return acc - comp;
+    }
+    return acc + blk;
+}
+
+// Sum over the voxels that detector row v's ray crosses of (t_exit - t_entry) *
+// f[voxel] (the projection divided by w), for the column path in spc (n pieces
+// from t_in to t_out), or with COUNT the row's number of (ray, voxel) pairs.
+// Called by whole warps.
+template <bool KAHAN, bool COUNT>
+__device__ __forceinline__ float column_row_sum(const ExactGeom& G, const ZParam* __restrict__ zp,
+                                                const float* __restrict__ volz, const float2* spc, int n, float t_in,
+                                                float t_out, int v, bool valid)
+{
+    ZParam Z;
+    Z.S = 0.0f;
+    Z.O = 0.0f;
+    Z.inv_S = 0.0f;
+    Z.kc = 0;
+    if (valid) Z = zp[v];
+    // the volume's bottom and top planes along this row's ray
+    const float z0 = plane_t(0, Z.S, Z.O, Z.kc), zZ = plane_t(G.Z, Z.S, Z.O, Z.kc);
+    const float t_lo = fminf(z0, zZ), t_hi = fmaxf(z0, zZ);
+    const float ta = fmaxf(t_in, t_lo), tb = fminf(t_out, t_hi);
+    const bool hit = valid && ta < tb;
+    int jb = INT_MAX, je = -1;
+    if (hit) {
+        jb = first_piece_ending<true>(spc, n, ta);
+        je = first_piece_ending<false>(spc, n, tb);
+    }
+    jb = __reduce_min_sync(0xffffffffu, jb);
+    je = __reduce_max_sync(0xffffffffu, je);
+    if (jb > je) return 0.0f;  // no row of the warp crosses the volume
+    const float t_start = (jb == 0) ? t_in : spc[jb - 1].x;
+    const float t_end = spc[je].x;
+    const int dk = Z.S > 0.0f ? 1 : -1;  // layer step along increasing t
+    // rows that miss the volume read the zero layer below their column and never cross
+    int kaddr = 0;
+    float kf = 0.0f, tzn = __int_as_float(0x7f800000);
+    if (hit) {
+        int plane;  // the next z plane the row crosses
+        if (t_start < t_lo) {  // outside, the volume ahead: the first plane is the near face
+            kaddr = dk > 0 ? 0 : G.Z + 1;
+            plane = dk > 0 ? 0 : G.Z;
+        } else {  // inside (t_start <= ta < tb <= t_hi)
+            const int k = locate<true>(t_start, Z.S, Z.O, Z.kc, G.Z, 1.0 / (double)Z.S);
+            kaddr = k + 1;
+            plane = dk > 0 ? k + 1 : k;
+        }
+        kf = (float)(plane - Z.kc);
+        tzn = fmaf(kf, Z.S, Z.O);
+    }
+    const int kexit = dk > 0 ? G.Z + 1 : 0;
+    const bool leaves = hit && t_start < t_hi && t_end > t_hi;  // crosses the far face within the pieces
+    const bool fast = !__any_sync(0xffffffffu, leaves);
+    const bool up = __all_sync(0xffffffffu, !hit || dk > 0);
+    const bool down = __all_sync(0xffffffffu, !hit || dk < 0);
+    if (fast) {
+        if (up) return walk_rows<KAHAN, true, 1, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, dk, kexit, G.Z);
+        if (down) return walk_rows<KAHAN, true, -1, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, dk, kexit, G.Z);
+        return walk_rows<KAHAN, true, 0, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, dk, kexit, G.Z);
+    }
+    if (up) return walk_rows<KAHAN, false, 1, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, dk, kexit, G.Z);
+    if (down) return walk_rows<KAHAN, false, -1, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, dk, kexit, G.Z);
+    return walk_rows<KAHAN, false, 0, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, dk, kexit, G.Z);
+}
+
+// MODE 0: out = projection (w * sum); MODE 1 (MLEM): out = w * g / Hf (0 where
+// Hf == 0), the Siddon back projector's input; MODE 2: out = g / Hf (the
+// voxel-driven back projector's); MODE 3: the (ray, voxel) pairs of positive
+// length are counted into out[0] (OT = unsigned long long).  g is read [view][v][u]; out is written in
+// the detector-column layout [view][u][v] when COLS (a warp's 32 rows store
+// 128 contiguous bytes), else [view][v][u].  A CTA takes detector column u of
+// one view and rows vstart .. vstart + kColRows - 1: from the tile list
+// {view, u | vstart << 16} (blockIdx.x indexes it) or, without one, u =
+// blockIdx.x, vstart = blockIdx.y * kColRows, view = view0 + blockIdx.z.
+template <bool KAHAN, int MODE, bool COLS, class GT, class OT>
+__global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const float4* __restrict__ txy,
+                                                             const int2* __restrict__ kxy,
+                                                             const ZParam* __restrict__ zp,
+                                                             const float* __restrict__ wq,
+                                                             const uint2* __restrict__ tiles, unsigned view0,
+                                                             const float* __restrict__ volz,
+                                                             const GT* __restrict__ g, OT* __restrict__ out)
+{
+    // piece j: {t where it ends, offset of its (x, y) voxel column in volz (int bits)}
+    extern __shared__ float2 spc[];
+    unsigned view;
+    int u, vstart;
+    if (tiles) {
+        const uint2 t = tiles[blockIdx.x];
+        view = t.x;
+        u = (int)(t.y & 0xffffu);
+        vstart = (int)(t.y >> 16);
+    } else {
+        view = view0 + blockIdx.z;
+        u = (int)blockIdx.x;
+        vstart = (int)blockIdx.y * kColRows;
+    }
+    const int Zp = G.Z + 2;
+    const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+    const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+    const float x0 = plane_t(0, T.x, T.y, K.x), x1 = plane_t(G.X, T.x, T.y, K.x);
+    const float y0 = plane_t(0, T.z, T.w, K.y), y1 = plane_t(G.Y, T.z, T.w, K.y);
+    const float t_in = fmaxf(fminf(x0, x1), fminf(y0, y1));
+    const float t_out = fminf(fmaxf(x0, x1), fmaxf(y0, y1));
+    int n = 0;  // pieces; 0 when the column's rays miss the volume's xy footprint
+    if (t_in < t_out) {
+        const double ivx = 1.0 / (double)T.x, ivy = 1.0 / (double)T.z;
+        const int ix = locate<true>(t_in, T.x, T.y, K.x, G.X, ivx), ex = locate<false>(t_out, T.x, T.y, K.x, G.X, ivx);
+        const int iy = locate<true>(t_in, T.z, T.w, K.y, G.Y, ivy), ey = locate<false>(t_out, T.z, T.w, K.y, G.Y, ivy);
+        const int nx = abs(ex - ix), ny = abs(ey - iy);
+        n = nx + ny + 1;
+        const int dx = T.x > 0.0f ? 1 : -1, dy = T.z > 0.0f ? 1 : -1;
+        // the first x and y planes crossed, relative to their kc
+        const int qx = (dx > 0 ? ix + 1 : ix) - K.x, qy = (dy > 0 ? iy + 1 : iy) - K.y;
+        const float isx = 1.0f / fabsf(T.x), isy = 1.0f / fabsf(T.z);
+        for (int q = threadIdx.x; q < nx + ny; q += blockDim.x) {
+            float t;
+            int pos, cx, cy;
+            if (q < nx) {  // x crossing q: after the y crossings strictly before it
+                t = fmaf((float)(qx + q * dx), T.x, T.y);
+                const int c = count_before<true>(t, qy, dy, T.z, T.w, isy, ny);
+                pos = q + c;
+                cx = ix + dx * (q + 1);
+                cy = iy + dy * c;
+            } else {  // y crossing b: after the x crossings at or before it
+                const int b = q - nx;
+                t = fmaf((float)(qy + b * dy), T.z, T.w);
+                const int c = count_before<false>(t, qx, dx, T.x, T.y, isx, nx);
+                pos = b + c;
+                cx = ix + dx * c;
+                cy = iy + dy * (b + 1);
+            }
+            spc[pos].x = t;                                        // piece pos ends here
+            spc[pos + 1].y = __int_as_float((cy * G.X + cx) * Zp);  // piece pos + 1 lies in (cx, cy)
+        }
+        if (threadIdx.x == 0) {
+            spc[0].y = __int_as_float((iy * G.X + ix) * Zp);
+            // the last piece ends at the first x or y plane after the exit voxel
+            spc[n - 1].x = fminf(fmaf((float)(qx + nx * dx), T.x, T.y), fmaf((float)(qy + ny * dy), T.z, T.w));
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (vstart + warp * 32 >= G.Nv) return;  // whole warps past the detector; no barrier follows
+    const int v = vstart + warp * 32 + lane;
+    const bool valid = v < G.Nv;
+    const float sum = (n > 0) ? column_row_sum<KAHAN, MODE == 3>(G, zp, volz, spc, n, t_in, t_out, v, valid) : 0.0f;
+    if (MODE == 3) {
+        unsigned long long c = valid ? (unsigned long long)sum : 0ull;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0 && c) atomicAdd(reinterpret_cast<unsigned long long*>(out), c);
+        return;
+    }
+    if (!valid) return;
+    if constexpr (MODE != 3) {
+    const size_t pix_rm = (size_t)v * G.Nu + u, pix_col = (size_t)u * G.Nv + v;
+    const size_t base = (size_t)(view - view0) * G.Nu * G.Nv;
+    const float w = __ldg(wq + pix_col);
+    const float hf = w * sum;
+    OT* const o = out + base + (COLS ? pix_col : pix_rm);
+    if (MODE == 0) {
+        store_val<OT>(o, hf);
+    } else {
+        const float gv = load_val<GT>(g + base + pix_rm);
+        const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
+        store_val<OT>(o, MODE == 1 ? ratio * w : ratio);
+    }
+    }
+}
+
+// f[z][y][x] -> volz[(y*X + x)*(Z + 2) + z + 1], 32 (x) x 32 (z) tiles of one y
+// through shared memory; the zero layers (z = -1 and z = Z) are set once when
+// the buffer is allocated and never written here.
+__global__ void __launch_bounds__(256) to_zfast_kernel(const float* __restrict__ in, float* __restrict__ out, int X,
+                                                       int Y, int Z)
+{
+    __shared__ float tile[32][33];
+    const int x0 = blockIdx.x * 32, z0 = blockIdx.y * 32, y = blockIdx.z;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int x = x0 + threadIdx.x, z = z0 + r;
+        if (x < X && z < Z) tile[r][threadIdx.x] = in[((size_t)z * Y + y) * X + x];
+    }
+    __syncthreads();
+    const size_t Zp = (size_t)Z + 2;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int z = z0 + threadIdx.x, x = x0 + r;
+        if (x < X && z < Z) out[((size_t)y * X + x) * Zp + z + 1] = tile[threadIdx.x][r];
+    }
+}
+
+}  // namespace exact
+
+// ---- host side -----------------------------------------------------------------------------
+
+// The column kernel needs every piece of a detector column's path to span less
+// than a voxel of z (0.9 at most: the column diagonal times the steepest row's
+// dz/dt, z being dz_v * (t + Rf) / R along row v's ray), int offsets into the
+// padded volume, u and row starts that fit 16 bits, and the path in shared memory.
+bool exact_fp_column_suits(const Plan& P)
+{
+    const ExactGeom& E = P.eg;
+    const double vx = E.vox[0], vy = E.vox[1], vz = E.vox[2];
+    if (!(vz > 0.0) || E.Ry == 0.0f) return false;
+    const double diag = std::sqrt(vx * vx + vy * vy);
+    const double slope = (0.5 * E.Nv * std::fabs((double)E.dv) + std::fabs((double)E.Dz)) / std::fabs((double)E.Ry);
+    const double needle = diag * slope / vz;
+    const double padded = (double)E.X * E.Y * (E.Z + 2.0);
+    return needle < 0.9 && padded < 2147483647.0 && E.Nu <= 65535 && E.Nv <= 65535 && E.Y <= 65535 &&
+           (size_t)(E.X + E.Y + 2) * sizeof(float2) <= 200 * 1024;
+}
+
+// Tiles {view, u | vstart << 16} of the column kernel: per view, the columns and
+// blocks of kColRows rows (from the first) inside the rectangle of rays that
+// cross the volume.  rect is per plan view {u_min, u_max, v_min, v_max}.
+recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect)
+{
+    const unsigned nv = P.nviews;
+    P.col_tiles.prefix.assign(nv + 1, 0);
+    std::vector<uint2> tiles;
+    for (unsigned n = 0; n < nv; ++n) {
+        P.col_tiles.prefix[n] = (unsigned)tiles.size();
+        const int4 r = rect[n];
+        if (r.y < r.x) continue;
+        for (int u = r.x; u <= r.y; ++u)
+            for (int vs = r.z; vs <= r.w; vs += exact::kColRows)
+                tiles.push_back(make_uint2(n, (unsigned)u | ((unsigned)vs << 16)));
+    }
+    P.col_tiles.prefix[nv] = (unsigned)tiles.size();
+    if (tiles.empty()) return RECON_OK;
+    RB_CHECK(P.alloc(&P.col_tiles.d, tiles.size(), "column tiles"));
+    RB_CUDA(cudaMemcpy(P.col_tiles.d, tiles.data(), tiles.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    return RECON_OK;
+}
+
+recon_status_t exact_to_zfast(const Plan& P, const float* vol, cudaStream_t s)
+{
+    const ExactGeom& E = P.eg;
+    exact::to_zfast_kernel<<<dim3((E.X + 31) / 32, (E.Z + 31) / 32, E.Y), dim3(32, 8), 0, s>>>(vol, P.d_vol_z, E.X,
+                                                                                             E.Y, E.Z);
+    RB_CUDA(cudaGetLastError());
+    return RECON_OK;
+}
+
+// Views [first, first + count) of table slots through the column kernel: the
+// tile list for plan views, the full grid otherwise (the scratch slot).  The
+// volume is copied to the z-fastest layout first.  For MODE 0 the pixels
+// outside the tiles are zeroed; the MLEM ratio buffers are zero there from
+// allocation on.
+template <int MODE, bool COLS, class GT, class OT>
+static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g, OT* out,
+                                    cudaStream_t s)
+{
+    if (count == 0) return RECON_OK;
+    const ExactGeom& E = P.eg;
+    dim3 grid;
+    const uint2* tiles = nullptr;
+    if (first + count <= P.nviews && P.col_tiles.prefix.size() == P.nviews + 1) {
+        const unsigned t0 = P.col_tiles.prefix[first], nt = P.col_tiles.prefix[first + count] - t0;
+        if (MODE == 0) RB_CUDA(cudaMemsetAsync(out, 0, (size_t)count * P.npix * sizeof(OT), s));
+        if (nt == 0) return RECON_OK;
+        grid = dim3(nt, 1, 1);
+        tiles = P.col_tiles.d + t0;
+    } else {
+        grid = dim3(E.Nu, (E.Nv + exact::kColRows - 1) / exact::kColRows, count);
+    }
+    if (MODE != 3) RB_CHECK(exact_to_zfast(P, vol, s));
+    const size_t smem = (size_t)(E.X + E.Y + 2) * sizeof(float2);
+    auto kernel = (P.opt.sum == RECON_SUM_KAHAN) ? exact::fp_column_kernel<true, MODE, COLS, GT, OT>
+                                                 : exact::fp_column_kernel<false, MODE, COLS, GT, OT>;
+    if (smem > 48 * 1024) RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kernel<<<grid, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, tiles, first, P.d_vol_z, g, out);
+    RB_CUDA(cudaGetLastError());
+    return RECON_OK;
+}
+
+// (ray, voxel) pairs of positive length over all plan views, as the column
+// kernel assigns them (synchronous; no volume is read).
+recon_status_t exact_fp_column_count(Plan& P, unsigned long long* total)
+{
+    unsigned long long* d = nullptr;
+    RB_CUDA(cudaMalloc(&d, sizeof(unsigned long long)));
+    cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
+    recon_status_t st = RECON_OK;
+    if (e == cudaSuccess) st = launch_column<3, false, float, unsigned long long>(P, nullptr, 0u, P.nviews, nullptr, d, 0);
+    if (e == cudaSuccess && st == RECON_OK) e = cudaMemcpy(total, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (st != RECON_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "column pair count");
+    return RECON_OK;
+}
+
+recon_status_t exact_fp_column(Plan& P, const float* vol, unsigned first, unsigned count, float* out, cudaStream_t s)
+{
+    return launch_column<0, false, float, float>(P, vol, first, count, nullptr, out, s);
+}
+
+// The MLEM ratio (MODE 1: times w, Siddon back projectors; MODE 2: without w,
+// voxel-driven) of views [first, first+count), written straight into the
+// layout its back projector reads.  g and ratio start at view `first`.
+recon_status_t exact_fp_column_ratio(Plan& P, const float* vol, const void* g, void* ratio, int mode, bool cols,
+                                     bool bf16, unsigned first, unsigned count, cudaStream_t s)
+{
+    using bf = __nv_bfloat16;
+    if (mode == 2) {
+        if (cols) return launch_column<2, true, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
+        return launch_column<2, false, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
+    }
+    if (bf16) {
+        if (cols) return launch_column<1, true, bf, bf>(P, vol, first, count, (const bf*)g, (bf*)ratio, s);
+        return launch_column<1, false, bf, bf>(P, vol, first, count, (const bf*)g, (bf*)ratio, s);
+    }
+    if (cols) return launch_column<1, true, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
+    return launch_column<1, false, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
+}
+
+}  // namespace rb

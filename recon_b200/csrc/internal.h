@@ -115,7 +115,10 @@ struct Plan {
     float* d_colsino = nullptr;  // a sinogram in the detector-column layout (gather back projector input)
     unsigned colsino_views = 0;   // views d_colsino holds
     bool bp_gather = false;    // Siddon back projection by the column gather (else ray-driven slabs)
-    float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y]
+    float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y] (ray-walk forward projector)
+    bool fp_column = false;    // forward projection by detector columns (fpcol.cu), else the ray walk
+    float* d_vol_z = nullptr;  // z-fastest copy of the projected volume with a zero layer at each end:
+                               // voxel (x, y, z) at [(y*X + x)*(Z + 2) + z + 1] (column forward projector)
     // back projection: fixed-point accumulators of one z-slab, image layout
     // and xy-transposed, and the max |value| of the call's input (float bits)
     unsigned long long* d_bpacc = nullptr;
@@ -124,6 +127,7 @@ struct Plan {
     // ray blocks crossing the volume (forward projection) and each
     // back-projection z-slab; rays outside them contribute nothing
     RayTiles fp_tiles;
+    RayTiles col_tiles;           // column forward projector: {view, u | vstart << 16} per CTA
     int4* d_view_rect = nullptr;  // [view] {u_min, u_max, v_min, v_max} of the rays crossing the volume
     std::vector<RayTiles> bp_tiles;
     TexCache tex;  // voxel-driven back projection
@@ -181,6 +185,8 @@ recon_status_t exact_fp(Plan& P, const float* vol, unsigned first, unsigned coun
 recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ratio, cudaStream_t s,
                               unsigned first, unsigned count);
 recon_status_t exact_count(Plan& P, unsigned long long* out);
+recon_status_t exact_bp_gather_count(Plan& P, unsigned long long* total);
+recon_status_t exact_fp_column_count(Plan& P, unsigned long long* total);
 // BP gather over views [first, first+count) of `sino` (weighted by w) into vol (overwrite);
 // sens_mode: back project ones; update: f = f*Ht/sens in the epilogue.
 recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, unsigned first,
@@ -218,6 +224,12 @@ int gather_slots(int Z);
 // layout [view][u][v].
 bool mlem_ratio_in_columns(const Plan& P);
 recon_status_t build_exact_culling(Plan& P);
+// forward projection by detector columns (fpcol.cu)
+bool exact_fp_column_suits(const Plan& P);
+recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect);
+recon_status_t exact_fp_column(Plan& P, const float* vol, unsigned first, unsigned count, float* out, cudaStream_t s);
+recon_status_t exact_fp_column_ratio(Plan& P, const float* vol, const void* g, void* ratio, int mode, bool cols,
+                                     bool bf16, unsigned first, unsigned count, cudaStream_t s);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);
 recon_status_t launch_update(float* f, const float* ht, const float* sens, size_t n, bool fast_div,
