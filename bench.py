@@ -367,7 +367,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from recon_b200 import SIDDON_BP_GATHER, SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN, Options, Plan
+    from recon_b200 import FP_COLUMNS, SIDDON_BP_GATHER, SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN, Options, Plan
     from recon_b200.configs import PLAIN_GPU
     from recon_b200.sharding import ordered_sum_, view_range
 
@@ -403,15 +403,18 @@ def main():
     first, count = view_range(nviews, rank, world)
     npix = P.nu * P.nv
     nvox = f.numel()
-    # kernels per step: transpose + forward; the gather back projector is one
-    # kernel after the ratio's transpose into detector columns, the ray-driven one
-    # maxabs + (ray + finish) per z-slab (both int64 accumulators of a slab in
-    # 64 MiB); at N > 1 a separate update
+    # kernels per step: the volume's copy (z-fastest for the column forward
+    # projector, xy-transposed for the ray walk) + the forward kernel; the gather
+    # back projector is one kernel (after the ratio's transpose into detector
+    # columns where the ray walk wrote it row-major), the ray-driven one maxabs +
+    # (ray + finish) per z-slab (both int64 accumulators of a slab in 64 MiB);
+    # at N > 1 a separate update
     gather = P.siddon_bp == SIDDON_BP_GATHER
+    columns = P.forward_projector == FP_COLUMNS
     Z, Y, X = P.shape_vol
     depth = max(1, min(Z, (64 << 20) // (X * Y * 16)))
     slabs = -(-Z // depth)
-    bp_launches = 2 if gather else 1 + 2 * slabs
+    bp_launches = (1 if columns else 2) if gather else 1 + 2 * slabs
 
     def iteration(ev=None):
         if world == 1:
@@ -539,6 +542,7 @@ def main():
         "isects_per_s": 2.0 * isects * value,
         "gpu_launches": args.steps * (2 + bp_launches + (0 if world == 1 else 1)),
         "back_projector": "gather" if gather else "ray",
+        "forward_projector": "detector columns" if columns else "ray walk",
     }
     peaks = {}
     try:
@@ -558,7 +562,8 @@ def main():
                    "back projection (maxabs + bp_ray_kernel per z-slab + bp_finish_kernel)", t_bp, bytes_bp,
                    traffic.get("bp"))
         else:
-            dom = ("forward projection (transpose_xy_kernel + fp_kernel)", t_fp, bytes_fp, traffic.get("fp"))
+            dom = ("forward projection (to_zfast_kernel + fp_column_kernel)" if columns else
+                   "forward projection (transpose_xy_kernel + fp_kernel)", t_fp, bytes_fp, traffic.get("fp"))
         ach = dom[2] / (dom[1] * 1e-3) / 1e9
         out["roofline"] = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": hbm, "unit": "GB/s",
                            "frac": ach / hbm, "peak_source": peak_src, "traffic": dom[3],

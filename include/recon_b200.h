@@ -170,6 +170,15 @@ size_t recon_plan_device_bytes(recon_plan_t plan);
  * RECON_SIDDON_BP_RAY, after the AUTO choice).  No counterpart in the
  * reference, which has one back projector. */
 recon_status_t recon_plan_siddon_bp(recon_plan_t plan, int* design);
+/* The forward projector an EXACT plan uses: RECON_FP_COLUMNS (the rays of one
+ * detector column share their (x, y) path, walked once per column; used where
+ * a ray's stretch in one (x, y) voxel column spans less than 0.9 voxel of z)
+ * or RECON_FP_RAY_WALK (one thread walks each ray).  Both give every (ray,
+ * voxel) pair the same length.  No counterpart in the reference, which has
+ * one forward projector. */
+#define RECON_FP_RAY_WALK 0
+#define RECON_FP_COLUMNS 1
+recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design);
 
 /* ---- projectors (device pointers, asynchronous on `stream`) ----------- */
 

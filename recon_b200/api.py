@@ -133,6 +133,13 @@ class Plan:
         check(lib().recon_plan_siddon_bp(self._h, C.byref(d)))
         return int(d.value)
 
+    @property
+    def forward_projector(self) -> int:
+        """The forward projector of an EXACT plan: FP_COLUMNS or FP_RAY_WALK."""
+        d = C.c_int(-1)
+        check(lib().recon_plan_forward_projector(self._h, C.byref(d)))
+        return int(d.value)
+
     # --- tensors ---
     def new_volume(self, fill: float = 0.0):
         import torch

@@ -301,6 +301,7 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             }
             RB_CHECK(build_exact_tables(*P, 0));
             RB_CHECK(build_exact_culling(*P));
+            if (P->bp_gather) RB_CHECK(exact_check_mirror(*P));
         } else {
             RB_CHECK(P->alloc(&P->d_maxabs, nv1, "maxabs"));
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));
@@ -325,6 +326,15 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
 void recon_plan_destroy(recon_plan_t plan) { delete plan; }
 
 size_t recon_plan_device_bytes(recon_plan_t plan) { return plan ? plan->device_bytes : 0; }
+
+recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design)
+{
+    if (!plan || !design) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (plan->opt.arith != RECON_ARITH_EXACT)
+        return fail(RECON_ERR_UNSUPPORTED, "COMPAT plans have a single forward projector");
+    *design = plan->fp_column ? RECON_FP_COLUMNS : RECON_FP_RAY_WALK;
+    return RECON_OK;
+}
 
 recon_status_t recon_plan_siddon_bp(recon_plan_t plan, int* design)
 {

@@ -194,13 +194,71 @@ struct GatherConst {
 };
 
 // A warp's column seen from one view: detector columns u_lo..u_hi and, for the
-// first two, the column's piece [A, B] of their rays and the row coefficients
-// ca = ez / (A + Rf), cb = ez / (B + Rf).
+// first two (sl = 0, 1), the column's piece [A, B] of their rays, the row
+// coefficients ca = ez / (A + Rf), cb = ez / (B + Rf) and the per-slot steps
+// pa = 32 vz ca, pb = 32 vz cb of the row bounds.  flags: bit sl = the rays of
+// u_lo + sl cross the column (A < B); bit 2 + sl = no voxel of the column has
+// a second candidate row there; bit 4 + sl = the piece lies behind the source
+// (every row is a candidate).
 struct GatherView {
+    float4 ab[2];  // {A, B, pa, pb}
+    float2 c[2];   // {ca, cb}
     int u_lo, u_hi;
-    float A[2], B[2], ca[2], cb[2];
-    unsigned single;  // bit sl: no voxel of the column has a second candidate row at u_lo + sl
+    unsigned flags;
 };
+
+// Column (i, j) of the volume, [Xa, Xb] x [Ya, Yb], seen from one view (see
+// GatherView); margin = the candidate rows' total widening (0.004 row).
+__device__ __forceinline__ GatherView gather_view(const ExactGeom& G, const GatherConst& C,
+                                                  const float4* __restrict__ txy, const int2* __restrict__ kxy,
+                                                  const float2* __restrict__ cs, unsigned view, int i, int j, float Xa,
+                                                  float Xb, float Ya, float Yb, float margin, float dz32)
+{
+    const float2 CS = __ldg(cs + view);
+    float umin = 3.0e38f, umax = -3.0e38f;
+    bool behind = false;
+#pragma unroll
+    for (int c4 = 0; c4 < 4; ++c4) {
+        const float X = (c4 & 1) ? Xb : Xa, Y = (c4 & 2) ? Yb : Ya;
+        const float a = X * CS.x - Y * CS.y, b = X * CS.y + Y * CS.x;
+        const float d = b + G.Rf;
+        behind |= !(d > 1e-3f * G.Rf);
+        const float uf = a / d * C.eu + C.ou;
+        umin = fminf(umin, uf);
+        umax = fmaxf(umax, uf);
+    }
+    GatherView V;
+    V.flags = 0u;
+    if (behind) {  // not for a volume in front of the source; stays exact anyway
+        V.u_lo = 0;
+        V.u_hi = G.Nu - 1;
+    } else {
+        V.u_lo = min(max(0, __float2int_ru(umin - 0.01f)), G.Nu);
+        V.u_hi = min(G.Nu - 1, __float2int_rd(umax + 0.01f));
+    }
+#pragma unroll
+    for (int sl = 0; sl < 2; ++sl) {
+        const int u = min(V.u_lo + sl, G.Nu - 1);
+        const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+        const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+        const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+        const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+        const float A = fmaxf(fminf(xa, xb), fminf(ya, yb));
+        const float B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+        const float ca = C.ez / (A + G.Rf), cb = C.ez / (B + G.Rf);
+        V.ab[sl] = make_float4(A, B, dz32 * ca, dz32 * cb);
+        V.c[sl] = make_float2(ca, cb);
+        if (A < B) V.flags |= 1u << sl;
+        // a voxel's candidate interval [f0, f1] (row units) has a length
+        // convex in its height, largest at the column's bottom or top voxel
+        const float zb = G.P0[2], zt = G.P0[2] + (float)G.Z * G.vox[2];
+        const float len_b = fmaxf((zb + G.vox[2]) * ca, (zb + G.vox[2]) * cb) - fminf(zb * ca, zb * cb);
+        const float len_t = fmaxf(zt * ca, zt * cb) - fminf((zt - G.vox[2]) * ca, (zt - G.vox[2]) * cb);
+        if (fmaxf(len_b, len_t) + margin < 0.99f) V.flags |= 1u << (2 + sl);
+        if (!(A + G.Rf > 1e-3f * G.Rf)) V.flags |= 1u << (4 + sl);
+    }
+    return V;
+}
 
 template <int EPI, class ST, int SLOTS>
 __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
@@ -256,172 +314,136 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
             acc[s] = 0.0f;
             acc2[s * 32 + lane] = 0.0f;
         }
-        {  // the views' contributions to this chunk
+        // the views' contributions to this chunk; SPLIT as `split`, a constant of
+        // the chunk's code
+        auto chunk = [&](auto split_tag) {
+            constexpr int SPLIT = decltype(split_tag)::value;
+            // detector column u of one view: its piece [A, B], row coefficients and
+            // steps; col = the view's values from row 0 of column u
+            auto piece = [&](float A, float B, float ca, float cb, float pa, float pb, bool single, bool behind,
+                             const ST* __restrict__ col) {
+                auto add = [&](int s, int v, float x) {
+                    const float4 zr = szq[v];
+                    const float t = fk0 + (float)(32 * s);
+                    const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                    const float L = fminf(B, hi) - fmaxf(A, lo);
+                    if (L > 0.0f) acc[s] = (EPI == 2) ? acc[s] + 1.0f : fmaf(L, x, acc[s]);
+                };
+                if (behind) {  // a piece behind the source: every row is a candidate
+#pragma unroll
+                    for (int s = 0; s < SLOTS; ++s)
+                        if (s < nslot)
+                            for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v));
+                    return;
+                }
+                // row bounds of slot s: f0 = min over the piece of the voxel's bottom
+                // row, f1 = max of its top row, both affine in s
+                const float P0a = fmaf(zl0, ca, oz_lo), P0b = fmaf(zl0, cb, oz_lo);
+                const float P1a = single ? 0.0f : fmaf(zh0, ca, oz_hi), P1b = single ? 0.0f : fmaf(zh0, cb, oz_hi);
+                // first candidate row of every voxel (loads issued together); a row that
+                // misses the voxel gives L <= 0 and adds nothing
+                auto first_rows = [&](auto single_tag) -> unsigned {
+                    constexpr bool SINGLE = decltype(single_tag)::value;
+                    unsigned more = 0u;
+                    int vl[SLOTS];
+                    decltype(load_raw(col)) x[SLOTS];
+#pragma unroll
+                    for (int s = 0; s < SLOTS; ++s) {
+                        // the lower of the two bounds: the piece's near end (a) for
+                        // voxels below the source plane, its far end (b) above it,
+                        // where the slot is on one side for every lane (SPLIT >= 0)
+                        const float f0 = SPLIT < 0 ? fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b))
+                                                   : (s < SPLIT ? fmaf((float)s, pa, P0a) : fmaf((float)s, pb, P0b));
+                        // clamped to a detector row, so every load is in bounds: a row
+                        // that is no candidate gives L <= 0, and the sums of slots past
+                        // the volume's top are never written out.  The conversion to
+                        // unsigned saturates (negative rows and NaN give 0), which leaves
+                        // one min for the clamp
+                        const int a = (int)min(__float2uint_ru(f0), (unsigned)G.Nv - 1u);
+                        vl[s] = a;
+                        x[s] = load_raw(col + a);
+                        if (!SINGLE) {  // the higher top bound: far end below z = 0, near end above
+                            const float f1 = SPLIT < 0
+                                                 ? fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b))
+                                                 : (s < SPLIT ? fmaf((float)s, pb, P1b) : fmaf((float)s, pa, P1a));
+                            if ((float)(a + 1) <= f1) more |= 1u << s;
+                        }
+                    }
+#pragma unroll
+                    for (int s = 0; s < SLOTS; ++s) add(s, vl[s], widen(x[s]));
+                    return more;
+                };
+                if (single) {
+                    first_rows(std::true_type{});
+                    return;
+                }
+                const unsigned more = first_rows(std::false_type{});
+                // further candidates (rare): summed apart, in shared memory
+                if (__any_sync(0xffffffffu, more != 0u)) {
+                    for (unsigned m = more; m != 0u; m &= m - 1u) {
+                        const int s = __ffs(m) - 1;
+                        const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
+                        const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                        const int a = max(0, __float2int_ru(f0));
+                        const int b = min(G.Nv - 1, __float2int_rd(f1));
+                        const float t = fk0 + (float)(32 * s);
+                        float sum = acc2[s * 32 + lane];
+                        for (int v = a + 1; v <= b; ++v) {
+                            const float4 zr = szq[v];
+                            const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                            const float L = fminf(B, hi) - fmaxf(A, lo);
+                            if (L > 0.0f) sum = (EPI == 2) ? sum + 1.0f : fmaf(L, load_val<ST>(col + v), sum);
+                        }
+                        acc2[s * 32 + lane] = sum;
+                    }
+                }
+            };
             for (unsigned vb = 0; vb < nview; vb += 32) {
                 const unsigned nb = min(32u, nview - vb);
-                if ((unsigned)lane < nb) {  // lane q sets up view vb + q
-                    const unsigned view = view0 + vb + lane;
-                    const float2 CS = __ldg(cs + view);
-                    float umin = 3.0e38f, umax = -3.0e38f;
-                    bool behind = false;
-#pragma unroll
-                    for (int c4 = 0; c4 < 4; ++c4) {
-                        const float X = (c4 & 1) ? Xb : Xa, Y = (c4 & 2) ? Yb : Ya;
-                        const float a = X * CS.x - Y * CS.y, b = X * CS.y + Y * CS.x;
-                        const float d = b + G.Rf;
-                        behind |= !(d > 1e-3f * G.Rf);
-                        const float uf = a / d * C.eu + C.ou;
-                        umin = fminf(umin, uf);
-                        umax = fmaxf(umax, uf);
-                    }
-                    GatherView V;
-                    V.single = 0u;
-                    if (behind) {  // not for a volume in front of the source; stays exact anyway
-                        V.u_lo = 0;
-                        V.u_hi = G.Nu - 1;
-                    } else {
-                        V.u_lo = min(max(0, __float2int_ru(umin - 0.01f)), G.Nu);
-                        V.u_hi = min(G.Nu - 1, __float2int_rd(umax + 0.01f));
-                    }
-#pragma unroll
-                    for (int sl = 0; sl < 2; ++sl) {
-                        const int u = min(V.u_lo + sl, G.Nu - 1);
-                        const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
-                        const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
-                        const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
-                        const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
-                        V.A[sl] = fmaxf(fminf(xa, xb), fminf(ya, yb));
-                        V.B[sl] = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
-                        V.ca[sl] = C.ez / (V.A[sl] + G.Rf);
-                        V.cb[sl] = C.ez / (V.B[sl] + G.Rf);
-                        // a voxel's candidate interval [f0, f1] (row units) has a length
-                        // convex in its height, largest at the column's bottom or top voxel
-                        const float zb = G.P0[2], zt = G.P0[2] + (float)G.Z * G.vox[2];
-                        const float len_b = fmaxf((zb + G.vox[2]) * V.ca[sl], (zb + G.vox[2]) * V.cb[sl]) -
-                                            fminf(zb * V.ca[sl], zb * V.cb[sl]);
-                        const float len_t = fmaxf(zt * V.ca[sl], zt * V.cb[sl]) -
-                                            fminf((zt - G.vox[2]) * V.ca[sl], (zt - G.vox[2]) * V.cb[sl]);
-                        if (fmaxf(len_b, len_t) + (oz_hi - oz_lo) < 0.99f) V.single |= 1u << sl;
-                    }
-                    sv[lane] = V;
-                }
+                if ((unsigned)lane < nb)  // lane q sets up view vb + q
+                    sv[lane] = gather_view(G, C, txy, kxy, cs, view0 + vb + lane, i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo,
+                                           dz32);
                 __syncwarp();
                 for (unsigned q = 0; q < nb; ++q) {
                     const unsigned vi = vb + q;
                     const int ulo = sv[q].u_lo, uhi = sv[q].u_hi;
-                    for (int u = ulo; u <= uhi; ++u) {
-                        const int sl = u - ulo;
-                        float A, B, ca, cb;
-                        if (sl < 2) {
-                            A = sv[q].A[sl];
-                            B = sv[q].B[sl];
-                            ca = sv[q].ca[sl];
-                            cb = sv[q].cb[sl];
-                        } else {  // a column wider than two detector pitches: set up here
-                            const unsigned view = view0 + vi;
-                            const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
-                            const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
-                            const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
-                            const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
-                            A = fmaxf(fminf(xa, xb), fminf(ya, yb));
-                            B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
-                            ca = C.ez / (A + G.Rf);
-                            cb = C.ez / (B + G.Rf);
-                        }
+                    const unsigned fl = sv[q].flags;
+                    // the first two detector columns, set up with the view
+#pragma unroll 1
+                    for (int sl = 0; sl < 2; ++sl) {
+                        if (ulo + sl > uhi) break;
+                        if (!((fl >> sl) & 1u)) continue;  // the rays miss the column
+                        const float4 ab = sv[q].ab[sl];
+                        const float2 cc = sv[q].c[sl];
+                        piece(ab.x, ab.y, cc.x, cc.y, ab.z, ab.w, (fl >> (2 + sl)) & 1u, (fl >> (4 + sl)) & 1u,
+                              vals + (size_t)vi * view_stride + (size_t)(ulo + sl) * G.Nv);
+                    }
+                    // a column wider than two detector pitches: set up here
+                    for (int u = ulo + 2; u <= uhi; ++u) {
+                        const unsigned view = view0 + vi;
+                        const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+                        const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+                        const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+                        const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+                        const float A = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                        const float B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
                         if (!(A < B)) continue;
-                        const ST* __restrict__ col = vals + (size_t)vi * view_stride + (size_t)u * G.Nv;
-                        auto add = [&](int s, int v, float x) {
-                            const float4 zr = szq[v];
-                            const float t = fk0 + (float)(32 * s);
-                            const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
-                            const float L = fminf(B, hi) - fmaxf(A, lo);
-                            if (L > 0.0f) acc[s] = (EPI == 2) ? acc[s] + 1.0f : fmaf(L, x, acc[s]);
-                        };
-                        if (!(A + G.Rf > 1e-3f * G.Rf)) {  // a piece behind the source: every row is a candidate
-#pragma unroll
-                            for (int s = 0; s < SLOTS; ++s)
-                                if (s < nslot)
-                                    for (int v = 0; v < G.Nv; ++v) add(s, v, load_val<ST>(col + v));
-                            continue;
-                        }
-                        // row bounds of slot s: f0 = min over the piece of the voxel's bottom
-                        // row, f1 = max of its top row, both affine in s
-                        const float pa = dz32 * ca, pb = dz32 * cb;
-                        const float P0a = fmaf(zl0, ca, oz_lo), P0b = fmaf(zl0, cb, oz_lo);
-                        const float P1a = fmaf(zh0, ca, oz_hi), P1b = fmaf(zh0, cb, oz_hi);
-                        // no voxel of the column with a second candidate (set up per view)
-                        const bool single = sl < 2 && ((sv[q].single >> sl) & 1u);
-                        // first candidate row of every voxel (loads issued together); a row that
-                        // misses the voxel gives L <= 0 and adds nothing
-                        unsigned more = 0u;
-                        auto first_rows = [&](auto single_tag, auto split_tag) {
-                            constexpr bool SINGLE = decltype(single_tag)::value;
-                            constexpr int SPLIT = decltype(split_tag)::value;
-                            int vl[SLOTS];
-                            decltype(load_raw(col)) x[SLOTS];
-#pragma unroll
-                            for (int s = 0; s < SLOTS; ++s) {
-                                // the lower of the two bounds: the piece's near end (a) for
-                                // voxels below the source plane, its far end (b) above it,
-                                // where the slot is on one side for every lane (SPLIT >= 0)
-                                const float f0 = SPLIT < 0 ? fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b))
-                                                           : (s < SPLIT ? fmaf((float)s, pa, P0a) : fmaf((float)s, pb, P0b));
-                                // clamped to a detector row, so every load is in bounds: a row
-                                // that is no candidate gives L <= 0, and the sums of slots past
-                                // the volume's top are never written out.  The conversion to
-                                // unsigned saturates (negative rows and NaN give 0), which leaves
-                                // one min for the clamp
-                                const int a = (int)min(__float2uint_ru(f0), (unsigned)G.Nv - 1u);
-                                vl[s] = a;
-                                x[s] = load_raw(col + a);
-                                if (!SINGLE) {  // the higher top bound: far end below z = 0, near end above
-                                    const float f1 =
-                                        SPLIT < 0 ? fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b))
-                                                  : (s < SPLIT ? fmaf((float)s, pb, P1b) : fmaf((float)s, pa, P1a));
-                                    if ((float)(a + 1) <= f1) more |= 1u << s;
-                                }
-                            }
-#pragma unroll
-                            for (int s = 0; s < SLOTS; ++s) add(s, vl[s], widen(x[s]));
-                        };
-                        auto rows = [&](auto single_tag) {
-                            if (SLOTS == 8 && split == 0)
-                                first_rows(single_tag, std::integral_constant<int, 0>{});
-                            else if (SLOTS == 8 && split == SLOTS / 2)
-                                first_rows(single_tag, std::integral_constant<int, SLOTS / 2>{});
-                            else if (SLOTS == 8 && split == SLOTS)
-                                first_rows(single_tag, std::integral_constant<int, SLOTS>{});
-                            else
-                                first_rows(single_tag, std::integral_constant<int, -1>{});
-                        };
-                        if (single)
-                            rows(std::true_type{});
-                        else
-                            rows(std::false_type{});
-                        // further candidates (rare): summed apart, in shared memory
-                        if (__any_sync(0xffffffffu, more != 0u)) {
-                            for (unsigned m = more; m != 0u; m &= m - 1u) {
-                                const int s = __ffs(m) - 1;
-                                const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
-                                const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
-                                const int a = max(0, __float2int_ru(f0));
-                                const int b = min(G.Nv - 1, __float2int_rd(f1));
-                                const float t = fk0 + (float)(32 * s);
-                                float sum = acc2[s * 32 + lane];
-                                for (int v = a + 1; v <= b; ++v) {
-                                    const float4 zr = szq[v];
-                                    const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
-                                    const float L = fminf(B, hi) - fmaxf(A, lo);
-                                    if (L > 0.0f) sum = (EPI == 2) ? sum + 1.0f : fmaf(L, load_val<ST>(col + v), sum);
-                                }
-                                acc2[s * 32 + lane] = sum;
-                            }
-                        }
+                        const float ca = C.ez / (A + G.Rf), cb = C.ez / (B + G.Rf);
+                        piece(A, B, ca, cb, dz32 * ca, dz32 * cb, false, !(A + G.Rf > 1e-3f * G.Rf),
+                              vals + (size_t)vi * view_stride + (size_t)u * G.Nv);
                     }
                 }
                 __syncwarp();  // the next batch rewrites sv
             }
-        }
+        };
+        if (SLOTS == 8 && split == 0)
+            chunk(std::integral_constant<int, 0>{});
+        else if (SLOTS == 8 && split == SLOTS / 2)
+            chunk(std::integral_constant<int, SLOTS / 2>{});
+        else if (SLOTS == 8 && split == SLOTS)
+            chunk(std::integral_constant<int, SLOTS>{});
+        else
+            chunk(std::integral_constant<int, -1>{});
         if (EPI == 2) {  // pair counts (exact: a voxel's count stays far below 2^24)
             unsigned long long c = 0;
 #pragma unroll
@@ -429,18 +451,224 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                 if (s < nslot) c += (unsigned long long)(acc[s] + acc2[s * 32 + lane]);
             for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
             if (lane == 0 && c) atomicAdd(npairs, c);
-            continue;
-        }
+        } else {
 #pragma unroll
-        for (int s = 0; s < SLOTS; ++s) {
-            if (s >= nslot) continue;
-            const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)(k0 + lane + 32 * s) * plane;
-            const float ht = acc[s] + acc2[s * 32 + lane];
-            if (EPI == 1) {
-                const float svv = sens[vox];
-                vol[vox] = (svv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[vox], ht), svv) : 0.0f;
-            } else {
-                vol[vox] = ht;
+            for (int s = 0; s < SLOTS; ++s) {
+                if (s >= nslot) continue;
+                const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)(k0 + lane + 32 * s) * plane;
+                const float ht = acc[s] + acc2[s * 32 + lane];
+                if (EPI == 1) {
+                    const float svv = sens[vox];
+                    vol[vox] = (svv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[vox], ht), svv) : 0.0f;
+                } else {
+                    vol[vox] = ht;
+                }
+            }
+        }
+    }
+}
+
+// The gather for geometries mirror-symmetric about the source plane z = 0: no
+// vertical detector offset, so row Nv-1-v's z planes are row v's mirrored,
+// bit for bit (S -> -S, O unchanged, kc -> Z - kc, checked on the plan's
+// table before this kernel is chosen).  Then row Nv-1-a gives voxel Z-1-k
+// exactly the length that row a gives voxel k: fmaf(-q, -S, O) = fmaf(q, S, O).
+// A lane owns the pairs (k, Z-1-k) for k = k0 + lane + 32 s < Z/2 (s < PS);
+// each pair's candidate rows and lengths are found once, for the lower voxel,
+// and each length is applied to both values, row a for voxel k and row
+// Nv-1-a for its mirror.  All the lower voxels lie below the source plane, so
+// a slot's row bounds come from one end of the piece each.  Sums, the sums'
+// order (views, detector columns, rows) and the epilogue are those of
+// bp_gather_kernel, so the results are deterministic too.
+template <int EPI, class ST, int PS>
+__global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_mirror_kernel(
+    ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
+    const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned view0, unsigned nview,
+    const ST* __restrict__ vals, size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens,
+    unsigned long long* __restrict__ npairs)
+{
+    extern __shared__ float4 szq[];  // as in bp_gather_kernel
+    __shared__ GatherView sview[kGatherWarps][32];
+    __shared__ float sacc2[kGatherWarps][2][PS * 32];  // further candidates: lower voxels, mirrors
+    for (int q = threadIdx.x; q < G.Nv; q += blockDim.x) {
+        const ZParam z = zp[q];
+        const float kc = (float)z.kc;
+        szq[q] = (z.S > 0.0f) ? make_float4(z.S, z.O, kc, kc - 1.0f) : make_float4(z.S, z.O, kc - 1.0f, kc);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kGatherTileX + warp % kGatherTileX;
+    const int j = blockIdx.y * (kGatherWarps / kGatherTileX) + warp / kGatherTileX;
+    if (i >= G.X || j >= G.Y) return;  // whole warps; no block barrier follows
+    GatherView* sv = sview[warp];
+    float* acc2 = sacc2[warp][0];
+    float* acc2m = sacc2[warp][1];
+    const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
+    const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
+    const size_t plane = (size_t)G.X * G.Y;
+    const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;  // margins as in bp_gather_kernel
+    const float dz32 = 32.0f * G.vox[2];
+    const int Zh = G.Z / 2;
+    const unsigned top = (unsigned)G.Nv - 1u;
+    for (int k0 = 0; k0 < Zh; k0 += 32 * PS) {
+        const float fk0 = (float)(k0 + lane);
+        const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
+        const int nslot = min(PS, max(0, (Zh - k0 - lane + 31) / 32));
+        float acc[PS], accm[PS];
+#pragma unroll
+        for (int s = 0; s < PS; ++s) {
+            acc[s] = 0.0f;
+            accm[s] = 0.0f;
+            acc2[s * 32 + lane] = 0.0f;
+            acc2m[s * 32 + lane] = 0.0f;
+        }
+        // detector column u of one view: its piece [A, B], row coefficients and
+        // steps; col = the view's values from row 0 of column u
+        auto piece = [&](float A, float B, float ca, float cb, float pa, float pb, bool single, bool behind,
+                         const ST* __restrict__ col) {
+            // row v's length through lower voxel s of this lane
+            auto length = [&](int s, int v) {
+                const float4 zr = szq[v];
+                const float t = fk0 + (float)(32 * s);
+                const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                return fminf(B, hi) - fmaxf(A, lo);
+            };
+            if (behind) {  // a piece behind the source: every row is a candidate
+#pragma unroll
+                for (int s = 0; s < PS; ++s)
+                    if (s < nslot)
+                        for (int v = 0; v < G.Nv; ++v) {
+                            const float L = length(s, v);
+                            if (L > 0.0f) {
+                                acc[s] = (EPI == 2) ? acc[s] + 1.0f : fmaf(L, load_val<ST>(col + v), acc[s]);
+                                accm[s] = (EPI == 2) ? accm[s] + 1.0f : fmaf(L, load_val<ST>(col + (top - v)), accm[s]);
+                            }
+                        }
+                return;
+            }
+            // row bounds of a lower voxel: f0 = its bottom row at the piece's near
+            // end, f1 = its top row at the far end (the voxel lies below z = 0)
+            const float P0a = fmaf(zl0, ca, oz_lo);
+            const float P1b = single ? 0.0f : fmaf(zh0, cb, oz_hi);
+            auto first_rows = [&](auto single_tag) -> unsigned {
+                constexpr bool SINGLE = decltype(single_tag)::value;
+                unsigned more = 0u;
+                int vl[PS];
+                decltype(load_raw(col)) x[PS], xm[PS];
+#pragma unroll
+                for (int s = 0; s < PS; ++s) {
+                    const float f0 = fmaf((float)s, pa, P0a);
+                    // clamped to a detector row: every load is in bounds, a row that
+                    // is no candidate has no positive length (see bp_gather_kernel)
+                    const unsigned a = min(__float2uint_ru(f0), top);
+                    vl[s] = (int)a;
+                    x[s] = load_raw(col + a);
+                    xm[s] = load_raw(col + (top - a));
+                    if (!SINGLE) {
+                        const float f1 = fmaf((float)s, pb, P1b);
+                        if ((float)(a + 1u) <= f1) more |= 1u << s;
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < PS; ++s) {
+                    const float L = length(s, vl[s]);
+                    if (L > 0.0f) {
+                        acc[s] = (EPI == 2) ? acc[s] + 1.0f : fmaf(L, widen(x[s]), acc[s]);
+                        accm[s] = (EPI == 2) ? accm[s] + 1.0f : fmaf(L, widen(xm[s]), accm[s]);
+                    }
+                }
+                return more;
+            };
+            if (single) {
+                first_rows(std::true_type{});
+                return;
+            }
+            const unsigned more = first_rows(std::false_type{});
+            // further candidates (rare): summed apart, in shared memory, over the
+            // bounds of both piece ends as bp_gather_kernel takes them
+            if (__any_sync(0xffffffffu, more != 0u)) {
+                const float P0b = fmaf(zl0, cb, oz_lo), P1a = fmaf(zh0, ca, oz_hi);
+                for (unsigned m = more; m != 0u; m &= m - 1u) {
+                    const int s = __ffs(m) - 1;
+                    const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
+                    const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                    const int a = max(0, __float2int_ru(f0));
+                    const int b = min(G.Nv - 1, __float2int_rd(f1));
+                    float sum = acc2[s * 32 + lane], summ = acc2m[s * 32 + lane];
+                    for (int v = a + 1; v <= b; ++v) {
+                        const float L = length(s, v);
+                        if (L > 0.0f) {
+                            sum = (EPI == 2) ? sum + 1.0f : fmaf(L, load_val<ST>(col + v), sum);
+                            summ = (EPI == 2) ? summ + 1.0f : fmaf(L, load_val<ST>(col + (top - v)), summ);
+                        }
+                    }
+                    acc2[s * 32 + lane] = sum;
+                    acc2m[s * 32 + lane] = summ;
+                }
+            }
+        };
+        for (unsigned vb = 0; vb < nview; vb += 32) {
+            const unsigned nb = min(32u, nview - vb);
+            if ((unsigned)lane < nb)  // lane q sets up view vb + q
+                sv[lane] = gather_view(G, C, txy, kxy, cs, view0 + vb + lane, i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo,
+                                       dz32);
+            __syncwarp();
+            for (unsigned q = 0; q < nb; ++q) {
+                const unsigned vi = vb + q;
+                const int ulo = sv[q].u_lo, uhi = sv[q].u_hi;
+                const unsigned fl = sv[q].flags;
+#pragma unroll 1
+                for (int sl = 0; sl < 2; ++sl) {
+                    if (ulo + sl > uhi) break;
+                    if (!((fl >> sl) & 1u)) continue;  // the rays miss the column
+                    const float4 ab = sv[q].ab[sl];
+                    const float2 cc = sv[q].c[sl];
+                    piece(ab.x, ab.y, cc.x, cc.y, ab.z, ab.w, (fl >> (2 + sl)) & 1u, (fl >> (4 + sl)) & 1u,
+                          vals + (size_t)vi * view_stride + (size_t)(ulo + sl) * G.Nv);
+                }
+                // a column wider than two detector pitches: set up here
+                for (int u = ulo + 2; u <= uhi; ++u) {
+                    const unsigned view = view0 + vi;
+                    const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+                    const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+                    const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+                    const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+                    const float A = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                    const float B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+                    if (!(A < B)) continue;
+                    const float ca = C.ez / (A + G.Rf), cb = C.ez / (B + G.Rf);
+                    piece(A, B, ca, cb, dz32 * ca, dz32 * cb, false, !(A + G.Rf > 1e-3f * G.Rf),
+                          vals + (size_t)vi * view_stride + (size_t)u * G.Nv);
+                }
+            }
+            __syncwarp();  // the next batch rewrites sv
+        }
+        if (EPI == 2) {  // pair counts
+            unsigned long long c = 0;
+#pragma unroll
+            for (int s = 0; s < PS; ++s)
+                if (s < nslot)
+                    c += (unsigned long long)(acc[s] + acc2[s * 32 + lane]) +
+                         (unsigned long long)(accm[s] + acc2m[s * 32 + lane]);
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0 && c) atomicAdd(npairs, c);
+        } else {
+#pragma unroll
+            for (int s = 0; s < PS; ++s) {
+                if (s >= nslot) continue;
+                const int k = k0 + lane + 32 * s;
+                const size_t col0 = (size_t)i + (size_t)j * G.X;
+                const size_t v0 = col0 + (size_t)k * plane, v1 = col0 + (size_t)(G.Z - 1 - k) * plane;
+                const float h0 = acc[s] + acc2[s * 32 + lane], h1 = accm[s] + acc2m[s * 32 + lane];
+                if (EPI == 1) {
+                    const float s0 = sens[v0], s1 = sens[v1];
+                    const float f0 = vol[v0], f1 = vol[v1];
+                    vol[v0] = (s0 != 0.0f) ? __fdiv_rn(__fmul_rn(f0, h0), s0) : 0.0f;
+                    vol[v1] = (s1 != 0.0f) ? __fdiv_rn(__fmul_rn(f1, h1), s1) : 0.0f;
+                } else {
+                    vol[v0] = h0;
+                    vol[v1] = h1;
+                }
             }
         }
     }
@@ -1051,12 +1279,36 @@ bool exact_bp_gather_suits(const Plan& P)
     return row_step >= 1.0 && row_step <= 1.4 && needle < 1.0 && E.Nv <= 3072 && E.Z >= 128;
 }
 
+// The gather may pair mirrored voxels (bp_gather_mirror_kernel) when the
+// volume has an even number of slices and the plan's z table is exactly
+// mirror-symmetric: row Nv-1-v has S = -S_v, O = O_v and kc = Z - kc_v, so
+// that its plane Z-k is row v's plane k bit for bit.  That holds with no
+// vertical detector offset (Dz = 0) and symmetric pixel centres; the table
+// itself is checked (synchronous, at plan creation).
+recon_status_t exact_check_mirror(Plan& P)
+{
+    P.bp_mirror = false;
+    if (P.eg.Z % 2 != 0 || P.eg.Z < 2) return RECON_OK;
+    std::vector<ZParam> z(P.eg.Nv);
+    RB_CUDA(cudaMemcpy(z.data(), P.d_zp, z.size() * sizeof(ZParam), cudaMemcpyDeviceToHost));
+    const int n = P.eg.Nv;
+    for (int v = 0; v < n; ++v) {
+        const ZParam& a = z[v];
+        const ZParam& b = z[n - 1 - v];
+        if (!(b.S == -a.S && b.O == a.O && b.kc == P.eg.Z - a.kc)) return RECON_OK;
+    }
+    P.bp_mirror = true;
+    return RECON_OK;
+}
+
 // Largest detector row count the gather back projector takes: its rows' z
 // planes are held in shared memory, 16 bytes per row, beside 18 KB of per-warp
 // arrays, within the 227 KB a block may use.
 int exact_bp_gather_max_rows() { return 12288; }
 
-template <int EPI, class ST, int SLOTS>
+// SLOTS: voxels per lane for bp_gather_kernel, voxel pairs per lane for the
+// mirror kernel (MIRROR).
+template <int EPI, class ST, int SLOTS, bool MIRROR = false>
 static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_stride, unsigned first,
                                           unsigned count, float* vol, const float* sens, cudaStream_t s,
                                           unsigned long long* npairs = nullptr)
@@ -1068,9 +1320,12 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
     C.ez = (float)((double)E.Ry / E.dv);
     C.oz = (float)(-((double)E.Dz + E.vd0) / E.dv);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
-    auto kernel = exact::bp_gather_kernel<EPI, ST, SLOTS>;
-    const size_t static_smem = sizeof(exact::GatherView) * 32 * exact::kGatherWarps +  // sview
-                               sizeof(float) * exact::kGatherWarps * SLOTS * 32;         // sacc2
+    auto kernel = [] {
+        if constexpr (MIRROR) return exact::bp_gather_mirror_kernel<EPI, ST, SLOTS>;
+        else return exact::bp_gather_kernel<EPI, ST, SLOTS>;
+    }();
+    const size_t static_smem = sizeof(exact::GatherView) * 32 * exact::kGatherWarps +          // sview
+                               sizeof(float) * exact::kGatherWarps * SLOTS * 32 * (MIRROR ? 2 : 1);  // sacc2
     if (smem + static_smem > 48 * 1024)
         RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
@@ -1090,11 +1345,28 @@ int gather_slots(int Z)
     return std::min(8, std::max(1, (Z + 32 * chunks - 1) / (32 * chunks)));
 }
 
+// Voxel pairs per lane for the mirror kernel: the lower half's height in as
+// few chunks of at most 4 x 32 slices as possible, split evenly.
+int gather_mirror_slots(int Z)
+{
+    const int half = Z / 2;
+    const int chunks = (half + 127) / 128;
+    return std::min(4, std::max(1, (half + 32 * chunks - 1) / (32 * chunks)));
+}
+
 template <int EPI, class ST>
 static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride, unsigned first, unsigned count,
                                     float* vol, const float* sens, cudaStream_t s,
                                     unsigned long long* npairs = nullptr)
 {
+    if (P.bp_mirror) {
+        switch (gather_mirror_slots(P.eg.Z)) {
+            case 1: return launch_gather_slots<EPI, ST, 1, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);
+            case 2: return launch_gather_slots<EPI, ST, 2, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);
+            case 3: return launch_gather_slots<EPI, ST, 3, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);
+            default: return launch_gather_slots<EPI, ST, 4, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);
+        }
+    }
 #define RB_GATHER_SLOTS(n) \
     case n: return launch_gather_slots<EPI, ST, n>(P, vals, view_stride, first, count, vol, sens, s, npairs)
     switch (gather_slots(P.eg.Z)) {
