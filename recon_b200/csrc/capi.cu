@@ -300,8 +300,8 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
                 RB_CUDA(cudaMemset(P->d_bpacc_t, 0, slab * sizeof(unsigned long long)));
             }
             RB_CHECK(build_exact_tables(*P, 0));
+            RB_CHECK(exact_check_mirror(*P));
             RB_CHECK(build_exact_culling(*P));
-            if (P->bp_gather) RB_CHECK(exact_check_mirror(*P));
         } else {
             RB_CHECK(P->alloc(&P->d_maxabs, nv1, "maxabs"));
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));

@@ -1279,15 +1279,17 @@ bool exact_bp_gather_suits(const Plan& P)
     return row_step >= 1.0 && row_step <= 1.4 && needle < 1.0 && E.Nv <= 3072 && E.Z >= 128;
 }
 
-// The gather may pair mirrored voxels (bp_gather_mirror_kernel) when the
-// volume has an even number of slices and the plan's z table is exactly
-// mirror-symmetric: row Nv-1-v has S = -S_v, O = O_v and kc = Z - kc_v, so
-// that its plane Z-k is row v's plane k bit for bit.  That holds with no
+// Both projectors pair mirrored rows / voxels (walk_rows_mirror,
+// bp_gather_mirror_kernel) when the volume has an even number of slices and
+// the plan's z table is exactly mirror-symmetric: row Nv-1-v has S = -S_v,
+// O = O_v and kc = Z - kc_v, so that its plane Z-k is row v's plane k bit for
+// bit, and the lower rows (v < Nv/2) descend along t.  That holds with no
 // vertical detector offset (Dz = 0) and symmetric pixel centres; the table
-// itself is checked (synchronous, at plan creation).
+// itself is checked (synchronous, at plan creation, before the culling that
+// lays out the forward projector's tiles).
 recon_status_t exact_check_mirror(Plan& P)
 {
-    P.bp_mirror = false;
+    P.z_mirror = false;
     if (P.eg.Z % 2 != 0 || P.eg.Z < 2) return RECON_OK;
     std::vector<ZParam> z(P.eg.Nv);
     RB_CUDA(cudaMemcpy(z.data(), P.d_zp, z.size() * sizeof(ZParam), cudaMemcpyDeviceToHost));
@@ -1296,8 +1298,9 @@ recon_status_t exact_check_mirror(Plan& P)
         const ZParam& a = z[v];
         const ZParam& b = z[n - 1 - v];
         if (!(b.S == -a.S && b.O == a.O && b.kc == P.eg.Z - a.kc)) return RECON_OK;
+        if (v < n / 2 && !(a.S < 0.0f)) return RECON_OK;  // lower rows descend along t
     }
-    P.bp_mirror = true;
+    P.z_mirror = true;
     return RECON_OK;
 }
 
@@ -1359,7 +1362,7 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
                                     float* vol, const float* sens, cudaStream_t s,
                                     unsigned long long* npairs = nullptr)
 {
-    if (P.bp_mirror) {
+    if (P.z_mirror) {
         switch (gather_mirror_slots(P.eg.Z)) {
             case 1: return launch_gather_slots<EPI, ST, 1, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);
             case 2: return launch_gather_slots<EPI, ST, 2, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);

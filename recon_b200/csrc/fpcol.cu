@@ -199,6 +199,124 @@ __device__ __forceinline__ float column_row_sum(const ExactGeom& G, const ZParam
     return walk_rows<KAHAN, false, 0, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, dk, kexit, G.Z);
 }
 
+// Rows mirrored about the source plane z = 0 (the plan's z table mirror-
+// symmetric: row Nv-1-v's plane Z-k is row v's plane k, bit for bit) cross
+// their z planes at the same t, so one lane walks lower row v (below z = 0,
+// its layer falling along t) and its mirror Nv-1-v together: one crossing
+// test and plane update, two loads and two sums.  The mirror's layer is
+// Z-1-k, at offset Z + 1 - kaddr of its padded column.  Returns {row v, row
+// Nv-1-v}.
+template <bool KAHAN, bool FAST, bool COUNT>
+__device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ volz, const float2* spc, int jb, int je,
+                                                   float cur, int kaddr, float kf, float tzn, float S, float O, int Z)
+{
+    const int zp1 = Z + 1;
+    float acc = 0.0f, comp = 0.0f, accm = 0.0f, compm = 0.0f, f1 = 0.0f, f1m = 0.0f;
+    auto piece = [&](int j, float& blk, float& blkm) {
+        const float2 pc = spc[j];
+        const float B = pc.x;
+        const int cb = __float_as_int(pc.y);
+        const float* p = volz + (cb + kaddr);
+        const float* pm = volz + (cb + (zp1 - kaddr));
+        const bool cross = tzn < B;
+        const float m = fminf(tzn, B);
+        if (COUNT) {  // layers 0 .. Z-1 sit at kaddr 1 .. Z, for both rows
+            const float in0 = (m - cur > 0.0f && (unsigned)(kaddr - 1) < (unsigned)Z) ? 1.0f : 0.0f;
+            const float in1 = (B - m > 0.0f && (unsigned)(kaddr - 2) < (unsigned)Z) ? 1.0f : 0.0f;
+            blk += in0 + in1;
+            blkm += in0 + in1;
+        } else {
+            const float f0 = __ldg(p), f0m = __ldg(pm);
+            if (cross) {
+                f1 = __ldg(p - 1);
+                f1m = __ldg(pm + 1);
+            }
+            const float L0 = m - cur, L1 = B - m;  // L1 = 0 without a crossing
+            blk = fmaf(L0, f0, blk);
+            blk = fmaf(L1, f1, blk);
+            blkm = fmaf(L0, f0m, blkm);
+            blkm = fmaf(L1, f1m, blkm);
+        }
+        if (cross) {
+            kaddr -= 1;
+            kf -= 1.0f;
+            tzn = fmaf(kf, S, O);
+            if (!FAST && kaddr == 0) tzn = __int_as_float(0x7f800000);  // left through the bottom
+        }
+        cur = B;
+    };
+    int j = jb;
+    for (; j + 7 <= je; j += 8) {
+        float blk = 0.0f, blkm = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) piece(j + q, blk, blkm);
+        if (KAHAN && !COUNT) {
+            kahan_add(acc, comp, blk);
+            kahan_add(accm, compm, blkm);
+        } else {
+            acc += blk;
+            accm += blkm;
+        }
+    }
+    float blk = 0.0f, blkm = 0.0f;
+#pragma unroll 1
+    for (; j <= je; ++j) piece(j, blk, blkm);
+    if (KAHAN && !COUNT) {
+        kahan_add(acc, comp, blk);
+        kahan_add(accm, compm, blkm);
+        return make_float2(acc - comp, accm - compm);
+    }
+    return make_float2(acc + blk, accm + blkm);
+}
+
+// column_row_sum for lower row v (v < Nv/2) and its mirror Nv-1-v.
+template <bool KAHAN, bool COUNT>
+__device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, const ZParam* __restrict__ zp,
+                                                        const float* __restrict__ volz, const float2* spc, int n,
+                                                        float t_in, float t_out, int v, bool valid)
+{
+    ZParam Z;
+    Z.S = 0.0f;
+    Z.O = 0.0f;
+    Z.inv_S = 0.0f;
+    Z.kc = 0;
+    if (valid) Z = zp[v];
+    const float z0 = plane_t(0, Z.S, Z.O, Z.kc), zZ = plane_t(G.Z, Z.S, Z.O, Z.kc);
+    const float t_lo = fminf(z0, zZ), t_hi = fmaxf(z0, zZ);  // the same for the mirror row
+    const float ta = fmaxf(t_in, t_lo), tb = fminf(t_out, t_hi);
+    const bool hit = valid && ta < tb;
+    int jb = INT_MAX, je = -1;
+    if (hit) {
+        jb = first_piece_ending<true>(spc, n, ta);
+        je = first_piece_ending<false>(spc, n, tb);
+    }
+    jb = __reduce_min_sync(0xffffffffu, jb);
+    je = __reduce_max_sync(0xffffffffu, je);
+    if (jb > je) return make_float2(0.0f, 0.0f);
+    const float t_start = (jb == 0) ? t_in : spc[jb - 1].x;
+    const float t_end = spc[je].x;
+    // lower rows descend along t (S < 0): their next plane is the layer's own
+    int kaddr = 0;
+    float kf = 0.0f, tzn = __int_as_float(0x7f800000);
+    if (hit) {
+        int plane;
+        if (t_start < t_lo) {  // above the volume: the first plane is the top face
+            kaddr = G.Z + 1;
+            plane = G.Z;
+        } else {
+            const int k = locate<true>(t_start, Z.S, Z.O, Z.kc, G.Z, 1.0 / (double)Z.S);
+            kaddr = k + 1;
+            plane = k;
+        }
+        kf = (float)(plane - Z.kc);
+        tzn = fmaf(kf, Z.S, Z.O);
+    }
+    const bool leaves = hit && t_start < t_hi && t_end > t_hi;
+    if (!__any_sync(0xffffffffu, leaves))
+        return walk_rows_mirror<KAHAN, true, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, G.Z);
+    return walk_rows_mirror<KAHAN, false, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, G.Z);
+}
+
 // MODE 0: out = projection (w * sum); MODE 1 (MLEM): out = w * g / Hf (0 where
 // Hf == 0), the Siddon back projector's input; MODE 2: out = g / Hf (the
 // voxel-driven back projector's); MODE 3: the (ray, voxel) pairs of positive
@@ -208,7 +326,9 @@ __device__ __forceinline__ float column_row_sum(const ExactGeom& G, const ZParam
 // one view and rows vstart .. vstart + kColRows - 1: from the tile list
 // {view, u | vstart << 16} (blockIdx.x indexes it) or, without one, u =
 // blockIdx.x, vstart = blockIdx.y * kColRows, view = view0 + blockIdx.z.
-template <bool KAHAN, int MODE, bool COLS, class GT, class OT>
+// MIRROR: rows come in mirrored pairs (see walk_rows_mirror); the CTA's rows
+// are lower rows (below Nv/2) and each lane also produces its mirror row.
+template <bool KAHAN, int MODE, bool COLS, class GT, class OT, bool MIRROR = false>
 __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                              const int2* __restrict__ kxy,
                                                              const ZParam* __restrict__ zp,
@@ -277,30 +397,39 @@ __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const 
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (vstart + warp * 32 >= G.Nv) return;  // whole warps past the detector; no barrier follows
+    const int vend = MIRROR ? G.Nv / 2 : G.Nv;  // rows this kernel walks (mirrors come with them)
+    if (vstart + warp * 32 >= vend) return;  // whole warps past them; no barrier follows
     const int v = vstart + warp * 32 + lane;
-    const bool valid = v < G.Nv;
-    const float sum = (n > 0) ? column_row_sum<KAHAN, MODE == 3>(G, zp, volz, spc, n, t_in, t_out, v, valid) : 0.0f;
+    const bool valid = v < vend;
+    float2 sum = make_float2(0.0f, 0.0f);
+    if (n > 0) {
+        if (MIRROR) sum = column_row_sum_mirror<KAHAN, MODE == 3>(G, zp, volz, spc, n, t_in, t_out, v, valid);
+        else sum.x = column_row_sum<KAHAN, MODE == 3>(G, zp, volz, spc, n, t_in, t_out, v, valid);
+    }
     if (MODE == 3) {
-        unsigned long long c = valid ? (unsigned long long)sum : 0ull;
+        unsigned long long c = valid ? (unsigned long long)sum.x + (unsigned long long)sum.y : 0ull;
         for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
         if (lane == 0 && c) atomicAdd(reinterpret_cast<unsigned long long*>(out), c);
         return;
     }
     if (!valid) return;
     if constexpr (MODE != 3) {
-    const size_t pix_rm = (size_t)v * G.Nu + u, pix_col = (size_t)u * G.Nv + v;
-    const size_t base = (size_t)(view - view0) * G.Nu * G.Nv;
-    const float w = __ldg(wq + pix_col);
-    const float hf = w * sum;
-    OT* const o = out + base + (COLS ? pix_col : pix_rm);
-    if (MODE == 0) {
-        store_val<OT>(o, hf);
-    } else {
-        const float gv = load_val<GT>(g + base + pix_rm);
-        const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-        store_val<OT>(o, MODE == 1 ? ratio * w : ratio);
-    }
+        const size_t base = (size_t)(view - view0) * G.Nu * G.Nv;
+        auto emit = [&](int row, float acc) {
+            const size_t pix_rm = (size_t)row * G.Nu + u, pix_col = (size_t)u * G.Nv + row;
+            const float w = __ldg(wq + pix_col);
+            const float hf = w * acc;
+            OT* const o = out + base + (COLS ? pix_col : pix_rm);
+            if (MODE == 0) {
+                store_val<OT>(o, hf);
+            } else {
+                const float gv = load_val<GT>(g + base + pix_rm);
+                const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
+                store_val<OT>(o, MODE == 1 ? ratio * w : ratio);
+            }
+        };
+        emit(v, sum.x);
+        if (MIRROR) emit(G.Nv - 1 - v, sum.y);
     }
 }
 
@@ -353,12 +482,16 @@ recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect)
     const unsigned nv = P.nviews;
     P.col_tiles.prefix.assign(nv + 1, 0);
     std::vector<uint2> tiles;
+    const int Nv = P.eg.Nv;
     for (unsigned n = 0; n < nv; ++n) {
         P.col_tiles.prefix[n] = (unsigned)tiles.size();
         const int4 r = rect[n];
         if (r.y < r.x) continue;
+        // mirror plans: the lower rows of the rectangle and of its mirror image
+        const int v0 = P.z_mirror ? std::min(r.z, Nv - 1 - r.w) : r.z;
+        const int v1 = P.z_mirror ? std::min(std::max(r.w, Nv - 1 - r.z), Nv / 2 - 1) : r.w;
         for (int u = r.x; u <= r.y; ++u)
-            for (int vs = r.z; vs <= r.w; vs += exact::kColRows)
+            for (int vs = v0; vs <= v1; vs += exact::kColRows)
                 tiles.push_back(make_uint2(n, (unsigned)u | ((unsigned)vs << 16)));
     }
     P.col_tiles.prefix[nv] = (unsigned)tiles.size();
@@ -397,12 +530,16 @@ static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, u
         grid = dim3(nt, 1, 1);
         tiles = P.col_tiles.d + t0;
     } else {
-        grid = dim3(E.Nu, (E.Nv + exact::kColRows - 1) / exact::kColRows, count);
+        const int rows = P.z_mirror ? E.Nv / 2 : E.Nv;
+        grid = dim3(E.Nu, (rows + exact::kColRows - 1) / exact::kColRows, count);
     }
     if (MODE != 3) RB_CHECK(exact_to_zfast(P, vol, s));
     const size_t smem = (size_t)(E.X + E.Y + 2) * sizeof(float2);
-    auto kernel = (P.opt.sum == RECON_SUM_KAHAN) ? exact::fp_column_kernel<true, MODE, COLS, GT, OT>
-                                                 : exact::fp_column_kernel<false, MODE, COLS, GT, OT>;
+    const bool kahan = P.opt.sum == RECON_SUM_KAHAN;
+    auto kernel = P.z_mirror ? (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, true>
+                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, true>)
+                             : (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, false>
+                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, false>);
     if (smem > 48 * 1024) RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kernel<<<grid, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, tiles, first, P.d_vol_z, g, out);
     RB_CUDA(cudaGetLastError());

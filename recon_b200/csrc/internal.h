@@ -115,7 +115,7 @@ struct Plan {
     float* d_colsino = nullptr;  // a sinogram in the detector-column layout (gather back projector input)
     unsigned colsino_views = 0;   // views d_colsino holds
     bool bp_gather = false;    // Siddon back projection by the column gather (else ray-driven slabs)
-    bool bp_mirror = false;    // the gather pairs voxels mirrored about z = 0 (z table mirror-symmetric)
+    bool z_mirror = false;     // z table mirror-symmetric about z = 0: both projectors pair mirrored rows/voxels
     float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y] (ray-walk forward projector)
     bool fp_column = false;    // forward projection by detector columns (fpcol.cu), else the ray walk
     float* d_vol_z = nullptr;  // z-fastest copy of the projected volume with a zero layer at each end:
