@@ -123,22 +123,29 @@ def gpu_index(local_rank: int) -> int:
     return local_rank
 
 
+DATA = ("synthetic (seeded 40-ellipsoid phantom in a 0.02/mm cylinder, Poisson noise I0=1e5 drawn view by view "
+        "from seed*100000+view)")
+
+
+def workload_config(args, world: int = 1) -> dict:
+    """The `config` of both arms' JSON lines."""
+    return {"workload": WORKLOAD, "volume": [256, 256, 256], "voxel_mm": 0.25, "views": 360,
+            "detector": [512, 512], "pixel_mm": 0.5, "arith": "exact", "sum": args.sum, "sino": args.sino,
+            "parallelism": f"views/{world}" if world > 1 else "single",
+            "l2": "no flush: per-step inputs (377 MB sinogram + 377 MB ratio) exceed the 126 MB L2"}
+
+
 def make_problem(cfg, device):
-    """Phantom and noisy measurement for the workload, built on the device."""
-    import torch
+    """Phantom and noisy measurement for the workload (recon_b200.phantom.workload):
+    the numpy phantom, projected by the EXACT projector on the device, Poisson
+    noise view by view on the host."""
+    from recon_b200.phantom import workload
 
-    from recon_b200 import Plan
-    from recon_b200.phantom import noisy, phantom
-
-    vol = torch.from_numpy(phantom(cfg)).to(device)
-    P0 = Plan(cfg)
-    p = P0.fp_views(vol)
-    g = noisy(p, cfg["I0"], cfg["seed"])
-    del p
-    return vol, g
+    return workload(cfg, device)
 
 
-TRAFFIC_PROFILE = "profiles/exact_fp_gather_bp_plain256_360v_512.md"
+TRAFFIC_PROFILE = "profiles/exact_fp_column_bp_mirror_plain256_360v_512.md"
+ACCURACY_PROFILE = "profiles/accuracy_plain256_360v_512.md"
 
 
 def measured_traffic() -> dict:
@@ -152,6 +159,38 @@ def measured_traffic() -> dict:
         return {}
     m = re.search(r"traffic-per-launch:\s*fp=(\d+)\s+bp=(\d+)", text)
     return {"fp": int(m.group(1)), "bp": int(m.group(2))} if m else {}
+
+
+def measured_accuracy() -> dict | None:
+    """Error of this workload against FP64, as the GPU accuracy test measured it
+    (committed summary, line `accuracy: {json}`): relative L2 of one MLEM update
+    against the FP64 update of the same image on the central 16 slices, at
+    iterations 1, 10 and 20, and the projectors' pair counts."""
+    import re
+
+    try:
+        text = open(os.path.join(ROOT, ACCURACY_PROFILE)).read()
+    except OSError:
+        return None
+    m = re.search(r"^accuracy:\s*(\{.*\})\s*$", text, re.M)
+    if not m:
+        return None
+    d = json.loads(m.group(1))
+    d["source"] = ACCURACY_PROFILE
+    return d
+
+
+def adjoint_check(P, seed: int = 7) -> float:
+    """|<Ax, y> - <x, A^T y>| / |<Ax, y>| for random x, y on the plan's own
+    projector pair (FP64 dot products of the FP32 results), measured in this run."""
+    import torch
+
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.rand(P.shape_vol, device="cuda", generator=gen)
+    y = torch.rand((P.nproj, P.nv, P.nu), device="cuda", generator=gen)
+    lhs = torch.dot(P.fp_views(x).double().ravel(), y.double().ravel()).item()
+    rhs = torch.dot(x.double().ravel(), P.bp_views(y).double().ravel()).item()
+    return abs(lhs - rhs) / abs(lhs)
 
 
 def shard_problems(work: list[float], world: int) -> list[list[int]]:
@@ -174,10 +213,13 @@ def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int
     are the max over ranks."""
     import torch
 
-    from recon_b200 import Batch, Plan
+    from recon_b200 import SIDDON_BP_GATHER, SIDDON_BP_TUNED, Batch, Options, Plan
     from recon_b200.configs import batched_problems
     from recon_b200.phantom import noisy, phantom
 
+    # both arms choose each problem's back projector by measurement
+    # (SIDDON_BP_TUNED, kept per geometry, so both make the same choice)
+    opts = Options(sum=opts.sum, sino=opts.sino, device=opts.device, siddon_bp=SIDDON_BP_TUNED)
     all_cfgs = batched_problems(n_prob, seed=4, iters=iters)
     work = [float(c["NumProj"]) * c["AxPixels"] * c["TAxPixels"] * (c["Xdim"] + c["Ydim"] + c["Zdim"])
             for c in all_cfgs]
@@ -210,6 +252,7 @@ def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int
     t_plain = e1.elapsed_time(e2) * 1e-3
     same = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(fb, fp))
     isects = sum(P.count_intersections() for P in plans)
+    n_gather = sum(1 for P in plans if P.siddon_bp == SIDDON_BP_GATHER)
     if world > 1:
         import torch.distributed as dist
 
@@ -226,6 +269,7 @@ def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int
         "batched_iter_s": n_prob * iters / t_batch, "plain_iter_s": n_prob * iters / t_plain,
         "speedup": t_plain / t_batch, "batched_isects_per_s": 2.0 * isects * iters / t_batch,
         "plain_isects_per_s": 2.0 * isects * iters / t_plain, "bitwise_equal": bool(same),
+        "back_projectors": {"gather": n_gather, "ray": len(plans) - n_gather, "choice": "measured per geometry"},
         "sharding": f"problems by rank over {world} GPUs" if world > 1 else "single GPU",
         "config": {"workload": f"batched_{n_prob}_seed4", "voxels_min_max": [min(vox), max(vox)],
                    "views_min_max": [min(int(c["NumProj"]) for c in cfgs), max(int(c["NumProj"]) for c in cfgs)],
@@ -301,6 +345,43 @@ def cpu_baseline(cfg, g_host, steps: int = 24):
                       f"scaled by (loopN+1)/(steps+1) to {t_view:.0f} s/view and by {n} views"}
 
 
+def reference_gpu_leg(O, geo, cfg, vol, gviews: dict) -> dict | None:
+    """The reference's own CUDA implementation on this GPU (its sources built for
+    sm_100a, oracle/_ref/libref_gpu.so), driven through its forward / backward
+    classes as its MLEM loop drives them per view (a_calc_initial_limits with
+    its blocking step-count read-back, the step-synchronous kernels, one view
+    in and one image out): FP then BP of the sampled views, extrapolated to the
+    360 views of an iteration.  The elementwise ratio and update kernels are
+    left out (a small part).  None when that build is missing."""
+    import numpy as np
+
+    R = O.ref_gpu()
+    if R is None:
+        return None
+    n = int(cfg["NumProj"])
+    dang = np.float32(cfg["DeltaAng"])
+    vol32 = vol.astype(np.float32)
+    img = np.zeros(geo.npix, np.float32)
+    bp = np.zeros(geo.nvox, np.float32)
+    R.ref_gpu_fp_view(geo, 0.0, vol32, img)  # context and module load
+    t_fp = t_bp = 0.0
+    views = sorted(gviews)
+    for v in views:
+        ang = float(np.float32(v) * dang)
+        t0 = time.perf_counter()
+        R.ref_gpu_fp_view(geo, ang, vol32, img)
+        t1 = time.perf_counter()
+        R.ref_gpu_bp_view(geo, ang, gviews[v], bp)
+        t2 = time.perf_counter()
+        t_fp += t1 - t0
+        t_bp += t2 - t1
+    per_view = (t_fp + t_bp) / len(views)
+    return {"value": 1.0 / (per_view * n), "unit": UNIT, "s_per_iteration": per_view * n,
+            "fp_s_per_view": t_fp / len(views), "bp_s_per_view": t_bp / len(views),
+            "sample": f"views {views}: forward and back projection each through the reference's classes, "
+                      f"extrapolated x{n}"}
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -330,33 +411,46 @@ def run_reference(args):
     dang = np.float32(cfg["DeltaAng"])
     nsample = max(1, args.steps + args.warmup)
     views = [int(round(k * n / nsample)) % n for k in range(nsample)]
+    # the GPU arm's inputs for these views: the same phantom, projected (here in
+    # FP64, there by the FP32 EXACT projector: equal to ~1e-7 relative) and the
+    # same Poisson draws (noisy_views: view n from seed * 100000 + n)
     gviews = {}
     for v in sorted(set(views)):
         img = np.zeros(geo.npix)
         O.lib().orc_x_fp_view(geo, float(np.float32(v) * dang), vol, img)
-        gviews[v] = noisy(img, cfg["I0"], cfg["seed"] + v).astype(np.float32)
+        gviews[v] = noisy(img, cfg["I0"], cfg["seed"] * 100000 + v).astype(np.float32)
     f = np.ones(geo.nvox, np.float32)
     ht = np.zeros(geo.nvox, np.float32)
-    times = []
+    times, sample_s = [], []
     prefix = 48
     for k, v in enumerate(views):
-        t_view, _, _, _ = ref_view_seconds(R, O, geo, cfg, v, prefix, f, gviews[v], ht)
+        t_view, dt, _, _ = ref_view_seconds(R, O, geo, cfg, v, prefix, f, gviews[v], ht)
         if k >= args.warmup:
             times.append(t_view)
+            sample_s.append(dt)
     tv = sum(times) / len(times)
     value = 1.0 / (tv * n)
     sample = (f"{len(times)} timed views (+{args.warmup} warm-up) of one MLEM iteration of the 256^3 / 360-view "
               f"workload with the reference's step-synchronous kernels built for the host on {threads} threads; "
               f"each view timed on the first {prefix} of its step launches and scaled by (loopN+1)/(steps+1) "
               f"(mean {tv:.1f} s/view), extrapolated x{n}")
-    print(json.dumps({
+    out = {
         **base, "value": value, "n_gpus": world, "steps": len(times), "warmup": args.warmup,
-        "ms_per_step": tv * n * 1e3, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded 40-ellipsoid phantom, Poisson I0=1e5)",
-        "config": {"workload": WORKLOAD, "volume": [256, 256, 256], "views": n, "detector": [512, 512]},
+        # a step is one sampled view's prefix of step launches: what was timed
+        "ms_per_step": 1e3 * sum(sample_s) / len(sample_s),
+        "extrapolated_ms_per_iteration": tv * n * 1e3,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": DATA,
+        "config": workload_config(args, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }))
+    }
+    try:
+        rg = reference_gpu_leg(O, geo, cfg, vol, {v: gviews[v] for v in sorted(set(views))[:4]})
+    except Exception as e:  # pragma: no cover
+        rg = {"error": str(e)}
+    if rg is not None:
+        out["reference_gpu"] = rg
+    print(json.dumps(out))
 
 
 def main():
@@ -369,7 +463,7 @@ def main():
 
     from recon_b200 import FP_COLUMNS, SIDDON_BP_GATHER, SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN, Options, Plan
     from recon_b200.configs import PLAIN_GPU
-    from recon_b200.sharding import ordered_sum_, view_range
+    from recon_b200.sharding import sharded_mlem_iteration, view_range
 
     world, rank, local = dist_env()
     if args.batched_only:
@@ -411,6 +505,7 @@ def main():
     # at N > 1 a separate update
     gather = P.siddon_bp == SIDDON_BP_GATHER
     columns = P.forward_projector == FP_COLUMNS
+    mirror = P.mirror_pairs
     Z, Y, X = P.shape_vol
     depth = max(1, min(Z, (64 << 20) // (X * Y * 16)))
     slabs = -(-Z // depth)
@@ -427,10 +522,7 @@ def main():
             if ev:
                 ev[2].record()
         else:
-            P.mlem_forward(g, f, first, count)
-            P.mlem_backward(ht, first, count)
-            ordered_sum_(ht)
-            P.mlem_update(f, ht)
+            sharded_mlem_iteration(P, g, f, ht)
 
     for _ in range(args.warmup):
         iteration()
@@ -533,16 +625,13 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f32" if args.sino == "f32" else "f32 (bf16 sinograms)",
-        "data": "synthetic (seeded 40-ellipsoid phantom in a 0.02/mm cylinder, Poisson noise I0=1e5)",
-        "config": {"workload": WORKLOAD, "volume": [256, 256, 256], "voxel_mm": 0.25, "views": nviews,
-                   "detector": [512, 512], "pixel_mm": 0.5, "arith": "exact",
-                   "sum": args.sum, "sino": args.sino, "parallelism": f"views/{world}" if world > 1 else "single",
-                   "l2": "no flush: per-step inputs (377 MB sinogram + 377 MB ratio) exceed the 126 MB L2"},
+        "data": DATA, "config": workload_config(args, world),
         "isects_per_pass": isects,
         "isects_per_s": 2.0 * isects * value,
         "gpu_launches": args.steps * (2 + bp_launches + (0 if world == 1 else 1)),
         "back_projector": "gather" if gather else "ray",
         "forward_projector": "detector columns" if columns else "ray walk",
+        "mirror_pairs": mirror,
     }
     peaks = {}
     try:
@@ -558,7 +647,8 @@ def main():
         bytes_bp = 4.0 * isects + 12.0 * nvox
         traffic = measured_traffic()
         if t_bp >= t_fp:
-            dom = ("back projection (bp_gather_kernel)" if gather else
+            dom = (("back projection (bp_gather_mirror_kernel)" if mirror else "back projection (bp_gather_kernel)")
+                   if gather else
                    "back projection (maxabs + bp_ray_kernel per z-slab + bp_finish_kernel)", t_bp, bytes_bp,
                    traffic.get("bp"))
         else:
@@ -575,6 +665,10 @@ def main():
                                      "fp_ms": t_fp, "bp_ms": t_bp}
     out["e2e"] = e2e
     out["clocks"] = clk
+    if world == 1:
+        acc = measured_accuracy() or {}
+        acc["adjoint_rel_this_run"] = adjoint_check(P)
+        out["accuracy"] = acc
     if world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(cfg, g_host.numpy().reshape(nviews, P.nv, P.nu),

@@ -15,7 +15,47 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "hf_siddon_class.hpp"
+
+namespace recon_b200 {
+// The COMPAT plan backward_projection samples through, kept between calls: a
+// reference-style caller back projects view after view with one geometry, and
+// building a plan (tables, accumulators) per call would dominate.  A new
+// geometry or device replaces it.  Like the reference's process-global
+// texture binding, this is one per process and not for concurrent use.
+struct voxel_bp_plan_cache {
+    recon_geometry_t geom{};
+    int device = -1;
+    recon_plan_t plan = nullptr;
+    ~voxel_bp_plan_cache()
+    {
+        if (plan) recon_plan_destroy(plan);
+    }
+    recon_plan_t get(const recon_geometry_t& g)
+    {
+        int dev = 0;
+        check_cuda(cudaGetDevice(&dev));
+        if (plan && dev == device && std::memcmp(&geom, &g, sizeof g) == 0) return plan;
+        if (plan) recon_plan_destroy(plan);
+        plan = nullptr;
+        recon_options_t o;
+        recon_default_options(&o);
+        o.arith = RECON_ARITH_COMPAT;
+        o.device = dev;
+        check(recon_plan_create(&g, &o, &plan));
+        geom = g;
+        device = dev;
+        return plan;
+    }
+    static voxel_bp_plan_cache& instance()
+    {
+        static voxel_bp_plan_cache c;
+        return c;
+    }
+};
+}  // namespace recon_b200
 
 struct texture_helper2D {
     float* m_image = nullptr;
@@ -58,7 +98,9 @@ struct texture_helper2D {
 // backward_projection (hf_cuda_kernels.cuh:183-237) for the image bound by the
 // last texture_helper2D::a2_input.  RM (the device rotation matrix) is taken
 // from the misalignment angles in CalParam.  `mode` selects the reference's
-// geometry (default) or the Siddon-consistent one.
+// geometry (default) or the Siddon-consistent one.  Asynchronous on the
+// legacy default stream, like the reference's kernel launch; the plan it runs
+// on is built on the first call for a geometry and kept (voxel_bp_plan_cache).
 inline void backward_projection(float* md_Obj, CalibrationParam CalParam, Detector Det, ObjectParam ObjParam,
                                 VoxVolParam voxparam, float* RM, float alpha, unsigned int Nprojections,
                                 int mode = RECON_VOXEL_REFERENCE)
@@ -68,14 +110,7 @@ inline void backward_projection(float* md_Obj, CalibrationParam CalParam, Detect
     texture_helper2D* t = texture_helper2D::current();
     if (!t || !t->m_image)
         throw recon_b200::config_error(RECON_ERR_INVALID_ARGUMENT, "no image bound (texture_helper2D::a2_input)");
-    recon_geometry_t g = recon_b200::make_geometry(CalParam, Det, voxparam);
-    recon_options_t o;
-    recon_default_options(&o);
-    o.arith = RECON_ARITH_COMPAT;
-    recon_plan_t plan = nullptr;
-    recon_b200::check(recon_plan_create(&g, &o, &plan));
-    recon_status_t s = recon_voxel_bp_view(plan, t->m_image, alpha, Nprojections, mode, md_Obj, nullptr);
-    cudaDeviceSynchronize();
-    recon_plan_destroy(plan);
-    recon_b200::check(s);
+    const recon_geometry_t g = recon_b200::make_geometry(CalParam, Det, voxparam);
+    recon_plan_t plan = recon_b200::voxel_bp_plan_cache::instance().get(g);
+    recon_b200::check(recon_voxel_bp_view(plan, t->m_image, alpha, Nprojections, mode, md_Obj, nullptr));
 }

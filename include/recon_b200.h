@@ -122,8 +122,18 @@ typedef enum { RECON_VOXEL_REFERENCE = 0, RECON_VOXEL_GEOMETRIC = 1 } recon_voxe
  *   AUTO   -- GATHER where the rays of adjacent rows cross a voxel column 1 to
  *     1.4 voxels apart (at the depth nearest the source), a ray's piece of one
  *     column spans less than a voxel of z, the volume is at least 128 voxels
- *     tall and the detector has at most 3072 rows; RAY otherwise. */
-typedef enum { RECON_SIDDON_BP_AUTO = 0, RECON_SIDDON_BP_GATHER = 1, RECON_SIDDON_BP_RAY = 2 } recon_siddon_bp_t;
+ *     tall and the detector has at most 3072 rows; RAY otherwise.
+ *   TUNED  -- measured: plan creation times a back projection with each
+ *     design on the plan's own geometry and keeps the faster.  The choice is
+ *     kept for the process per geometry and device, so every plan of that
+ *     geometry (a batch's and a plain one alike) makes the same choice and
+ *     gives the same bits.  recon_plan_siddon_bp reports it. */
+typedef enum {
+    RECON_SIDDON_BP_AUTO = 0,
+    RECON_SIDDON_BP_GATHER = 1,
+    RECON_SIDDON_BP_RAY = 2,
+    RECON_SIDDON_BP_TUNED = 3
+} recon_siddon_bp_t;
 
 typedef struct {
     int arith;      /* recon_arith_t, default EXACT */
@@ -179,6 +189,13 @@ recon_status_t recon_plan_siddon_bp(recon_plan_t plan, int* design);
 #define RECON_FP_RAY_WALK 0
 #define RECON_FP_COLUMNS 1
 recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design);
+/* *paired = 1 when the plan's EXACT projectors take detector rows (and, in
+ * the gather back projector, voxels) in pairs mirrored about the source plane
+ * z = 0, computing each pair's shared lengths once: where the volume has an
+ * even slice count and the FP64-built z table is exactly mirror-symmetric
+ * (no vertical detector offset Dz).  Results are the same either way.  No
+ * counterpart in the reference. */
+recon_status_t recon_plan_mirror_pairs(recon_plan_t plan, int* paired);
 
 /* ---- projectors (device pointers, asynchronous on `stream`) ----------- */
 
@@ -363,8 +380,10 @@ recon_status_t recon_view_step_count(recon_plan_t plan, float angle_deg, unsigne
  *  - volumes above RECON_NOALLOC_MAX_VOXELS voxels return RECON_ERR_UNSUPPORTED;
  *  - overlapping calls on one device (other streams or host threads) share
  *    the scratch and corrupt each other; calls in one stream are safe;
- *  - the first call on a device looks up the scratch address: make it before
- *    capturing a stream into a CUDA graph.
+ *  - the first call on a device looks up the scratch address and keeps it for
+ *    the life of the process: make it before capturing a stream into a CUDA
+ *    graph, and do not call this entry point after a cudaDeviceReset of that
+ *    device (the kept address no longer belongs to the new context).
  * Uses the current device; asynchronous on `stream`. */
 #define RECON_NOALLOC_MAX_VOXELS 2097152
 recon_status_t recon_compat_bp_view_noalloc(const recon_geometry_t* geom, const float* d_img,

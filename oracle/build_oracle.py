@@ -6,8 +6,9 @@
 * ``oracle/_ref/libref_gpu.so`` -- the reference's own CUDA sources built with
   nvcc for sm_100a (ref_gpu_harness.cu + shims).
 
-The reference sources are compiled where they lie (``REFERENCE_SRC``); nothing
-is copied.  The two reference builds only run where that directory exists
+The reference sources are compiled where they lie (``REFERENCE_SRC``: the
+environment variable RECON_REFERENCE_SRC, else ``CT_Recon`` of a checkout of
+the reference named ``reference`` beside this repository); nothing is copied.  The two reference builds only run where that directory exists
 (the development container); elsewhere the prebuilt ``.so`` files are used.
 Outputs go to ``oracle/`` and ``oracle/_ref/`` only.
 """
@@ -20,7 +21,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
-REFERENCE_SRC = os.environ.get("RECON_REFERENCE_SRC", "/root/reference/CT_Recon")
+REFERENCE_SRC = os.environ.get("RECON_REFERENCE_SRC",
+                               os.path.normpath(os.path.join(HERE, "..", "..", "reference", "CT_Recon")))
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -146,7 +146,11 @@ def ref_gpu():
         L.ref_gpu_mlem_cfg.argtypes = [C.c_char_p, C.c_char_p]
         L.ref_gpu_mlem_cfg.restype = C.c_float
         L.ref_gpu_forward_projection_cfg.argtypes = [C.c_char_p, C.c_char_p]
+        if hasattr(L, "ref_gpu_backward_projection_cfg"):
+            L.ref_gpu_backward_projection_cfg.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
         L.ref_gpu_voxel_bp2_view.argtypes = [_GP, C.c_float, _f32p, C.c_uint, _f32p]
+        if hasattr(L, "ref_gpu_march_fp_view"):
+            L.ref_gpu_march_fp_view.argtypes = [_GP, C.c_float, _f32p, _f32p]
         _ref_gpu = L
     return _ref_gpu
 

@@ -1,7 +1,7 @@
 /*
  * ref_cpu_harness.cpp -- host build of the reference's own Siddon kernels.
  *
- * CHECKER / BASELINE INFRASTRUCTURE.  Built by oracle/build_ref.py from the
+ * CHECKER / BASELINE INFRASTRUCTURE.  Built by oracle/build_oracle.py from the
  * reference sources where they lie (no copies), with the prelude
  * oracle/ref_shim/host_cuda/ref_prelude_cpu.h forced in, into
  * oracle/_ref/libref_cpu.so.  Two uses:

@@ -17,6 +17,7 @@
  */
 #include "hf_siddon_recon.hpp"
 
+#include <cmath>
 #include <cstdint>
 #include <vector>
 
@@ -219,6 +220,16 @@ void ref_gpu_forward_projection_cfg(const char* folder, const char* cfg)
     recon.a1_FORWARD_PROJECTION(std::string(folder), std::string(cfg));
 }
 
+/* siddon_recon::a1_BACKWARD_PROJECTION (hf_siddon_recon.hpp:165-182).  Its total
+ * image accumulates into md_f, which m_recon_initiate allocates without
+ * clearing (hf_siddon_recon.hpp:425, 568); the per-view images
+ * (write_per_angle) start from cleared memory (hf_siddon_class.hpp:318). */
+void ref_gpu_backward_projection_cfg(const char* folder, const char* cfg, int write_per_angle)
+{
+    siddon_recon recon;
+    recon.a1_BACKWARD_PROJECTION(std::string(folder), std::string(cfg), write_per_angle != 0);
+}
+
 /* backward_projection2 (hf_cuda_kernels.cuh:240-284) for one view, added
  * into vol.  The device image is padded by two rows and two pixels so the
  * kernel's inclusive upper-edge taps stay inside the allocation (they read
@@ -244,6 +255,46 @@ void ref_gpu_voxel_bp2_view(const orc_geom* g, float angle, const float* img, un
     CUDA_SAFE_CALL(cudaMemcpy(vol, d_vol, V * 4, cudaMemcpyDeviceToHost));
     CUDA_SAFE_CALL(cudaFree(d_img));
     CUDA_SAFE_CALL(cudaFree(d_vol));
+    CUDA_SAFE_CALL(cudaFree(d_RM));
+}
+
+/* forward_projection (hf_cuda_kernels.cuh:126-180), the reference's texture
+ * ray-marching projector, for one view: the reference gives no loop over
+ * depths, so it is launched once per depth y0 = L((k + 1/2)/Ydim - 1/2),
+ * k < Ydim, L = (Ydim - 1) YVoxSize (the normalised texel centres along y),
+ * adding into a cleared image, with the volume bound to the tex3D stand-in of
+ * ref_prelude_gpu.h.  Launch shape as its other image kernels (4 x 4 threads,
+ * hf_siddon_recon.hpp:368-371). */
+void ref_gpu_march_fp_view(const orc_geom* g, float angle, const float* vol, float* img)
+{
+    RefGeom G(g);
+    const size_t V = (size_t)g->Xdim * g->Ydim * g->Zdim;
+    const size_t N = (size_t)g->NumAxPixels * g->NumTAxPixels;
+    float *d_vol, *d_img, *d_RM;
+    CUDA_SAFE_CALL(cudaMalloc((void**)&d_vol, V * 4));
+    CUDA_SAFE_CALL(cudaMemcpy(d_vol, vol, V * 4, cudaMemcpyHostToDevice));
+    CUDA_SAFE_CALL(cudaMalloc((void**)&d_img, N * 4));
+    CUDA_SAFE_CALL(cudaMemset(d_img, 0, N * 4));
+    CUDA_SAFE_CALL(cudaMalloc((void**)&d_RM, 9 * 4));
+    rotation_matrix3D(d_RM, G.cp.xangle, G.cp.yangle, G.cp.zangle); /* hf_cuda_functions.cuh:66-88 */
+    const int dims[3] = {(int)g->Xdim, (int)g->Ydim, (int)g->Zdim};
+    const float* bound = d_vol;
+    CUDA_SAFE_CALL(cudaMemcpyToSymbol(recon_ref_tex3_dims, dims, sizeof dims));
+    CUDA_SAFE_CALL(cudaMemcpyToSymbol(recon_ref_tex3_data, &bound, sizeof bound));
+    ObjectParam op;
+    op.ObjX = op.ObjY = op.ObjZ = op.ObjXangle = op.ObjYangle = op.ObjZangle = 0.f;
+    const float L = ((float)g->Ydim - 1.0f) * g->YVoxSize;
+    const float step = L / (float)g->Ydim, first = L * (0.5f / (float)g->Ydim - 0.5f);
+    for (unsigned k = 0; k < g->Ydim; ++k) {
+        const float y0 = std::fma((float)k, step, first);
+        forward_projection<<<G.bimg, G.timg>>>(d_img, G.cp, G.det, op, G.vox, d_RM, y0, angle);
+    }
+    CUDA_SAFE_CALL(cudaGetLastError());
+    CUDA_SAFE_CALL(cudaMemcpy(img, d_img, N * 4, cudaMemcpyDeviceToHost));
+    bound = nullptr;
+    CUDA_SAFE_CALL(cudaMemcpyToSymbol(recon_ref_tex3_data, &bound, sizeof bound));
+    CUDA_SAFE_CALL(cudaFree(d_vol));
+    CUDA_SAFE_CALL(cudaFree(d_img));
     CUDA_SAFE_CALL(cudaFree(d_RM));
 }
 

@@ -23,7 +23,7 @@ SUM_KAHAN, SUM_PLAIN = 0, 1
 SINO_F32, SINO_BF16 = 0, 1
 BP_SIDDON, BP_VOXEL = 0, 1
 VOXEL_REFERENCE, VOXEL_GEOMETRIC = 0, 1
-SIDDON_BP_AUTO, SIDDON_BP_GATHER, SIDDON_BP_RAY = 0, 1, 2
+SIDDON_BP_AUTO, SIDDON_BP_GATHER, SIDDON_BP_RAY, SIDDON_BP_TUNED = 0, 1, 2, 3
 NOALLOC_MAX_VOXELS = 2097152  # RECON_NOALLOC_MAX_VOXELS
 PROJECTOR_FORWARD = 0  # RECON_PROJECTOR_FORWARD
 PROJECTOR_BACK = 1  # RECON_PROJECTOR_BACK
@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
         "recon_plan_device_bytes": (C.c_size_t, [P]),
         "recon_plan_siddon_bp": (st, [P, ip]),
         "recon_plan_forward_projector": (st, [P, C.POINTER(C.c_int)]),
+        "recon_plan_mirror_pairs": (st, [P, C.POINTER(C.c_int)]),
         "recon_march_fp_view": (st, [P, P, f, C.c_int, P, P]),
         "recon_fp_view": (st, [P, P, f, P, P]),
         "recon_fp_views": (st, [P, P, u, u, P, P]),
@@ -148,7 +149,7 @@ def exported_symbols() -> list[str]:
     """Names of the C ABI functions this binding expects (all of include/recon_b200.h)."""
     return [
         "recon_abi_version", "recon_last_error", "recon_default_options", "recon_geometry_from_cfg",
-        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_fp_view", "recon_fp_views",
+        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_plan_mirror_pairs", "recon_fp_view", "recon_fp_views",
         "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_march_fp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_count_projector_pairs", "recon_set_ones", "recon_divide1", "recon_multiply1",

@@ -134,6 +134,13 @@ class Plan:
         return int(d.value)
 
     @property
+    def mirror_pairs(self) -> bool:
+        """True when the EXACT projectors pair rows / voxels mirrored about z = 0."""
+        d = C.c_int(0)
+        check(lib().recon_plan_mirror_pairs(self._h, C.byref(d)))
+        return bool(d.value)
+
+    @property
     def forward_projector(self) -> int:
         """The forward projector of an EXACT plan: FP_COLUMNS or FP_RAY_WALK."""
         d = C.c_int(-1)
@@ -324,7 +331,19 @@ def compat_bp_view_noalloc(cfg: dict, img, angle: float, out):
     `out` on the current CUDA device, with no device allocation by the library
     (at most L.NOALLOC_MAX_VOXELS voxels; overlapping calls on one device
     share its scratch and must not run concurrently)."""
+    import torch
+
     g = geometry(cfg)
+    nv, nu = int(cfg["TAxPixels"]), int(cfg["AxPixels"])
+    shape_vol = (int(cfg["Zdim"]), int(cfg["Ydim"]), int(cfg["Xdim"]))
+    dev = torch.cuda.current_device()
+    for name, t, shape in (("img", img, (nv, nu)), ("out", out, shape_vol)):
+        if not isinstance(t, torch.Tensor) or t.dtype != torch.float32 or not t.is_cuda:
+            raise ValueError(f"{name} must be a float32 CUDA tensor")
+        if t.device.index != dev:
+            raise ValueError(f"{name} is on cuda:{t.device.index}, the current device is cuda:{dev}")
+        if tuple(t.shape) != shape or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous {shape} tensor, got {tuple(t.shape)}")
     check(lib().recon_compat_bp_view_noalloc(C.byref(g), _ptr(img), float(angle), _ptr(out), _stream()))
     return out
 

@@ -72,7 +72,7 @@ static recon_status_t validate(const recon_geometry_t& g, const recon_options_t&
     if (o.voxel_mode != RECON_VOXEL_REFERENCE && o.voxel_mode != RECON_VOXEL_GEOMETRIC)
         return fail(RECON_ERR_INVALID_ARGUMENT, "unknown voxel_mode option");
     if (o.siddon_bp != RECON_SIDDON_BP_AUTO && o.siddon_bp != RECON_SIDDON_BP_GATHER &&
-        o.siddon_bp != RECON_SIDDON_BP_RAY)
+        o.siddon_bp != RECON_SIDDON_BP_RAY && o.siddon_bp != RECON_SIDDON_BP_TUNED)
         return fail(RECON_ERR_INVALID_ARGUMENT, "unknown siddon_bp option");
     if (o.arith == RECON_ARITH_EXACT) {
         if (c.xangle != 0.0f || c.yangle != 0.0f || c.zangle != 0.0f)
@@ -277,7 +277,10 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(P->alloc(&P->d_cs, nv1, "view trig"));
             RB_CHECK(P->alloc(&P->d_zp, geom->det.NumTAxPixels, "ray table z"));
             RB_CHECK(P->alloc(&P->d_w, P->npix, "ray weights"));
-            P->bp_gather = opt.siddon_bp == RECON_SIDDON_BP_GATHER ||
+            // TUNED: both designs are set up, timed below and the slower one's
+            // accumulators released (exact_tune_bp)
+            const bool tuned = opt.siddon_bp == RECON_SIDDON_BP_TUNED && P->eg.Nv <= exact_bp_gather_max_rows();
+            P->bp_gather = opt.siddon_bp == RECON_SIDDON_BP_GATHER || tuned ||
                            (opt.siddon_bp == RECON_SIDDON_BP_AUTO && exact_bp_gather_suits(*P));
             RB_CHECK(P->alloc(&P->d_wq, P->npix, "ray weights (detector columns)"));
             RB_CUDA(cudaMemset(P->d_wq, 0, P->npix * sizeof(float)));
@@ -291,7 +294,7 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             } else {
                 RB_CHECK(P->alloc(&P->d_vol_t, P->nvox, "transposed volume"));
             }
-            if (!P->bp_gather) {  // the ray-driven back projector's slab accumulators
+            if (!P->bp_gather || tuned) {  // the ray-driven back projector's slab accumulators
                 const size_t slab = (size_t)P->eg.X * P->eg.Y * bp_slab_depth(*P);
                 RB_CHECK(P->alloc(&P->d_bpacc, slab, "back projection accumulator"));
                 RB_CHECK(P->alloc(&P->d_bpacc_t, slab, "back projection accumulator (transposed)"));
@@ -301,7 +304,9 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             }
             RB_CHECK(build_exact_tables(*P, 0));
             RB_CHECK(exact_check_mirror(*P));
+            if (tuned) P->bp_gather = false;  // the culling builds the ray design's slab tiles too
             RB_CHECK(build_exact_culling(*P));
+            if (tuned) RB_CHECK(exact_tune_bp(*P));
         } else {
             RB_CHECK(P->alloc(&P->d_maxabs, nv1, "maxabs"));
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));
@@ -333,6 +338,13 @@ recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design)
     if (plan->opt.arith != RECON_ARITH_EXACT)
         return fail(RECON_ERR_UNSUPPORTED, "COMPAT plans have a single forward projector");
     *design = plan->fp_column ? RECON_FP_COLUMNS : RECON_FP_RAY_WALK;
+    return RECON_OK;
+}
+
+recon_status_t recon_plan_mirror_pairs(recon_plan_t plan, int* paired)
+{
+    if (!plan || !paired) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    *paired = (plan->opt.arith == RECON_ARITH_EXACT && plan->z_mirror) ? 1 : 0;
     return RECON_OK;
 }
 

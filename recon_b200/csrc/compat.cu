@@ -348,8 +348,12 @@ __global__ void fp_kernel(CompatGeom G, const float* __restrict__ angles, const 
         float gv = g[n];
         float ratio = (acc != 0) ? __fdividef(gv, acc) : 0.0f;
         out[n] = ratio;
-        unsigned bits = __float_as_uint(fabsf(ratio));
-        if (bits) atomicMax(&maxabs[view], bits);
+        // one atomic per warp: every ray of the block belongs to this view, and a
+        // max does not depend on the order it is taken in
+        const unsigned active = __activemask();
+        const unsigned bits = __reduce_max_sync(active, __float_as_uint(fabsf(ratio)));
+        const unsigned lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31u;
+        if (bits && (active & ((1u << lane) - 1u)) == 0u) atomicMax(&maxabs[view], bits);
     }
 }
 

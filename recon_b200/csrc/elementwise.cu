@@ -51,15 +51,39 @@ __global__ void fill_kernel(float* __restrict__ a, float v, size_t n)
 // f = f * Ht; f = divide1(f, sens) (hf_siddon_recon.hpp:473-474), two roundings
 // in that order.  fast_div: the reference's __fdividef; else IEEE division.
 template <bool FAST>
+__device__ __forceinline__ float update_one(float f, float ht, float s)
+{
+    const float p = __fmul_rn(f, ht);
+    return (s != 0.0f) ? (FAST ? __fdividef(p, s) : __fdiv_rn(p, s)) : 0.0f;
+}
+
+// 128-bit loads and stores where all three arrays are 16-byte aligned.
+template <bool FAST>
 __global__ void update_kernel(float* __restrict__ f, const float* __restrict__ ht, const float* __restrict__ sens,
                               size_t n)
 {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += stride) {
-        const float p = __fmul_rn(f[q], ht[q]);
-        const float s = sens[q];
-        f[q] = (s != 0.0f) ? (FAST ? __fdividef(p, s) : __fdiv_rn(p, s)) : 0.0f;
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const bool aligned =
+        ((reinterpret_cast<uintptr_t>(f) | reinterpret_cast<uintptr_t>(ht) | reinterpret_cast<uintptr_t>(sens)) & 15) == 0;
+    size_t q0 = 0;
+    if (aligned) {
+        const size_t n4 = n / 4;
+        float4* f4 = reinterpret_cast<float4*>(f);
+        const float4* h4 = reinterpret_cast<const float4*>(ht);
+        const float4* s4 = reinterpret_cast<const float4*>(sens);
+        for (size_t q = i; q < n4; q += stride) {
+            float4 x = f4[q];
+            const float4 h = __ldg(h4 + q), sv = __ldg(s4 + q);
+            x.x = update_one<FAST>(x.x, h.x, sv.x);
+            x.y = update_one<FAST>(x.y, h.y, sv.y);
+            x.z = update_one<FAST>(x.z, h.z, sv.z);
+            x.w = update_one<FAST>(x.w, h.w, sv.w);
+            f4[q] = x;
+        }
+        q0 = n4 * 4;
     }
+    for (size_t q = q0 + i; q < n; q += stride) f[q] = update_one<FAST>(f[q], ht[q], sens[q]);
 }
 
 static unsigned blocks_for(size_t n)

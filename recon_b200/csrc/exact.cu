@@ -32,6 +32,10 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
 #include <type_traits>
 
 namespace rb {
@@ -1301,6 +1305,88 @@ recon_status_t exact_check_mirror(Plan& P)
         if (v < n / 2 && !(a.S < 0.0f)) return RECON_OK;  // lower rows descend along t
     }
     P.z_mirror = true;
+    return RECON_OK;
+}
+
+// RECON_SIDDON_BP_TUNED: the design a plan of this geometry (on this device)
+// measured faster, kept for the process so that every plan of the geometry
+// makes the same choice.
+namespace {
+std::mutex g_bp_tune_mutex;
+std::map<std::string, bool> g_bp_tune_gather;
+
+std::string bp_tune_key(const Plan& P)
+{
+    const recon_geometry_t& g = P.geom;
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "%d|%a %a %a %a %a %a|%u %u %a %a|%u %u %u %a %a %a|%u %a", P.device, g.cal.R,
+                  g.cal.Rf, g.cal.Ry, g.cal.Dx, g.cal.Dz, g.cal.M, g.det.NumTAxPixels, g.det.NumAxPixels,
+                  g.det.TAxPixDimMm, g.det.AxPixDimMm, g.vox.Xdim, g.vox.Ydim, g.vox.Zdim, g.vox.XVoxSize,
+                  g.vox.YVoxSize, g.vox.ZVoxSize, g.scan.NumProj, g.scan.DeltaAng);
+    return buf;
+}
+
+void release(Plan& P, void* p, size_t bytes)
+{
+    if (!p) return;
+    cudaFree(p);
+    P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), p));
+    P.device_bytes -= bytes;
+}
+}  // namespace
+
+// Times the plan's sensitivity back projection (all views, both designs set up
+// by the plan) with each design, CUDA events around the second of two runs on
+// the legacy stream, and keeps the faster; the ray design's slab accumulators
+// are released when the gather wins.  Synchronous (plan creation).
+recon_status_t exact_tune_bp(Plan& P)
+{
+    const std::string key = bp_tune_key(P);
+    bool known = false, gather = true;
+    {
+        std::lock_guard<std::mutex> lock(g_bp_tune_mutex);
+        auto it = g_bp_tune_gather.find(key);
+        if (it != g_bp_tune_gather.end()) {
+            known = true;
+            gather = it->second;
+        }
+    }
+    if (!known && P.nviews > 0) {
+        float* out = nullptr;
+        RB_CUDA(cudaMalloc(&out, P.nvox * sizeof(float)));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaError_t e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        float ms[2] = {0.0f, 0.0f};
+        recon_status_t st = RECON_OK;
+        for (int d = 0; d < 2 && e == cudaSuccess && st == RECON_OK; ++d) {
+            P.bp_gather = (d == 0);
+            st = exact_bp(P, nullptr, false, false, 0, P.nviews, false, true, out, nullptr, nullptr, 0);
+            if (st == RECON_OK) e = cudaEventRecord(e0, 0);
+            if (e == cudaSuccess && st == RECON_OK)
+                st = exact_bp(P, nullptr, false, false, 0, P.nviews, false, true, out, nullptr, nullptr, 0);
+            if (e == cudaSuccess && st == RECON_OK) e = cudaEventRecord(e1, 0);
+            if (e == cudaSuccess && st == RECON_OK) e = cudaEventSynchronize(e1);
+            if (e == cudaSuccess && st == RECON_OK) e = cudaEventElapsedTime(&ms[d], e0, e1);
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        cudaFree(out);
+        if (st != RECON_OK) return st;
+        if (e != cudaSuccess) return cuda_fail(e, "back projector tuning");
+        gather = ms[0] <= ms[1];
+        std::lock_guard<std::mutex> lock(g_bp_tune_mutex);
+        g_bp_tune_gather.emplace(key, gather);
+    }
+    P.bp_gather = gather;
+    if (gather) {
+        const size_t slab = (size_t)P.eg.X * P.eg.Y * bp_slab_depth(P) * sizeof(unsigned long long);
+        release(P, P.d_bpacc, slab);
+        release(P, P.d_bpacc_t, slab);
+        release(P, P.d_bpmax, sizeof(unsigned));
+        P.d_bpacc = P.d_bpacc_t = nullptr;
+        P.d_bpmax = nullptr;
+    }
     return RECON_OK;
 }
 

@@ -226,6 +226,7 @@ int gather_slots(int Z);
 bool mlem_ratio_in_columns(const Plan& P);
 recon_status_t build_exact_culling(Plan& P);
 recon_status_t exact_check_mirror(Plan& P);
+recon_status_t exact_tune_bp(Plan& P);
 // forward projection by detector columns (fpcol.cu)
 bool exact_fp_column_suits(const Plan& P);
 recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect);

@@ -15,7 +15,8 @@
 // Here one thread follows one ray through all its depths in registers:
 //   REFERENCE: the kernel's arithmetic as written (pixel_iterate without
 //     rounding, the misalignment matrix, __fdividef, the angle in radians with
-//     the reference's M_PI; its sine and cosine computed once on the host),
+//     the reference's M_PI and its sine and cosine from the device's sincosf,
+//     hf_cuda_kernels.cuh:146-147),
 //     depths at the texel centres of the normalised y coordinate,
 //     y0 = L·((k + 1/2)/Ydim - 1/2) for k = 0..Ydim-1, and the texel a
 //     normalised, point-filtered, border-addressed tex3D returns:
@@ -41,11 +42,13 @@ struct MarchGeom {
     float L;        // (Ydim - 1) * YVoxSize
     int nplanes;    // depths y0 = y_first + k * y_step
     float y_first, y_step;
+    float angle_deg;  // REFERENCE: the view angle, turned into sine and cosine on the device
 };
 
 template <int MODE>
 __global__ void __launch_bounds__(128) march_fp_kernel(MarchGeom G, float c, float s, const float* __restrict__ vol,
                                                         float* __restrict__ img)
+// c, s: cosine and sine of the view angle (GEOMETRIC; REFERENCE computes its own)
 {
     const int u = blockIdx.x * 32 + threadIdx.x, v = blockIdx.y * 4 + threadIdx.y;
     if (u >= G.Nu || v >= G.Nv) return;
@@ -63,6 +66,11 @@ __global__ void __launch_bounds__(128) march_fp_kernel(MarchGeom G, float c, flo
         u_id = G.R / den * (G.RM[0] * pu + G.RM[2] * pv + G.Dx);
         v_id = G.R / den * (G.RM[6] * pu + G.RM[8] * pv + G.Dz);
         w = sqrtf(v_id * v_id + u_id * u_id + G.R * G.R) / G.R * G.y_step;
+    }
+    if (MODE == RECON_VOXEL_REFERENCE) {
+        // sincosf(alpha_deg * (float)M_PI / 180.0f) with #define M_PI 3.1415927
+        // (hf_cuda_kernels.cuh:23, 146-147)
+        sincosf(G.angle_deg * 3.1415927f / 180.0f, &s, &c);
     }
     const size_t plane = (size_t)G.X * G.Y;
     float acc = 0.0f;
@@ -134,14 +142,13 @@ recon_status_t march_fp_view(Plan& P, const float* vol, float angle_deg, int mod
     G.dv = g.det.TAxPixDimMm;
     for (int i = 0; i < 9; ++i) G.RM[i] = P.RM[i];
     G.L = ((float)G.Y - 1.0f) * G.vox[1];
+    G.angle_deg = angle_deg;
     float c, sn;
     if (mode == RECON_VOXEL_REFERENCE) {
         G.nplanes = G.Y;
         G.y_step = G.L / (float)G.Y;
         G.y_first = G.L * (0.5f / (float)G.Y - 0.5f);
-        const float a = angle_deg * 3.1415927f / 180.0f;  // #define M_PI, hf_cuda_kernels.cuh:23
-        sn = std::sin(a);
-        c = std::cos(a);
+        sn = c = 0.0f;  // the kernel takes sincosf of angle_deg itself
     } else {
         const double hx = 0.5 * G.X * G.vox[0], hy = 0.5 * G.Y * G.vox[1];
         const double r = std::sqrt(hx * hx + hy * hy);

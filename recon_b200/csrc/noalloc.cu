@@ -17,7 +17,9 @@
 //    different host threads) race on it and corrupt each other's result.
 //    Calls in one stream are ordered and safe;
 //  * the first call on a device looks up the scratch address (and may load
-//    the library's device code), so make it before any stream capture.
+//    the library's device code), so make it before any stream capture; the
+//    address is kept for the process's life, so the entry point must not be
+//    called after a cudaDeviceReset of that device.
 #include <cmath>
 #include <mutex>
 

@@ -157,3 +157,38 @@ def noisy(p, I0: float, seed: int, clip: bool = True):
     if clip:
         g = np.maximum(g, 0.0)
     return g.astype(np.float32)
+
+
+def noisy_views(p, I0: float, seed: int, clip: bool = True):
+    """noisy() view by view on the host: view n of p ([view][v][u], numpy array
+    or torch tensor) is drawn from the seed ``seed * 100000 + n``, so that any
+    subset of views can be reproduced without the others.  Returns the type
+    (and device) of p."""
+    try:
+        import torch
+
+        if isinstance(p, torch.Tensor):
+            host = p.detach().cpu().numpy()
+            out = np.stack([noisy(host[n], I0, seed * 100000 + n, clip) for n in range(host.shape[0])])
+            return torch.from_numpy(out).to(p.device)
+    except ImportError:
+        pass
+    p = np.asarray(p)
+    return np.stack([noisy(p[n], I0, seed * 100000 + n, clip) for n in range(p.shape[0])])
+
+
+def workload(cfg: dict, device, host_phantom: bool = True):
+    """The measured workload of a preset: its phantom (voxelised on the host
+    with numpy, or on `device` when host_phantom is False), forward projected
+    by the EXACT projector of a default plan on `device`, with Poisson noise
+    view by view (noisy_views).  Returns (volume, sinogram) as device tensors."""
+    import torch
+
+    from .api import Plan
+
+    dev = torch.device(device)
+    vol = torch.from_numpy(phantom(cfg)).to(dev) if host_phantom else phantom(cfg, device=dev)
+    p = Plan(cfg).fp_views(vol)
+    g = noisy_views(p, cfg["I0"], cfg["seed"])
+    del p
+    return vol, g

@@ -10,8 +10,6 @@ call).  Then every rank applies the same update.  Over NCCL on NVLink this is
 """
 from __future__ import annotations
 
-from typing import Callable
-
 import torch
 import torch.distributed as dist
 
@@ -23,6 +21,23 @@ def view_range(nviews: int, rank: int, world: int) -> tuple[int, int]:
     return first, base + (1 if rank < rem else 0)
 
 
+# Exchange buffers of ordered_sum_, kept per (size, dtype, device, world): an
+# MLEM run sums one image per iteration, always of the same size.
+_buffers: dict = {}
+
+
+def _exchange_buffers(n: int, dtype, device, world: int):
+    key = (n, dtype, str(device), world)
+    buf = _buffers.get(key)
+    if buf is None:
+        per = (n + world - 1) // world
+        padded = torch.zeros(per * world, dtype=dtype, device=device)  # the tail past n stays zero
+        buf = (padded, torch.empty_like(padded), torch.empty(per, dtype=dtype, device=device),
+               torch.empty_like(padded))
+        _buffers[key] = buf
+    return buf
+
+
 def ordered_sum_(t: torch.Tensor, group=None) -> torch.Tensor:
     """In-place sum of `t` over all ranks, accumulated in rank order 0..N-1."""
     world = dist.get_world_size(group)
@@ -30,39 +45,33 @@ def ordered_sum_(t: torch.Tensor, group=None) -> torch.Tensor:
         return t
     flat = t.reshape(-1)
     n = flat.numel()
-    per = (n + world - 1) // world
-    padded = torch.zeros(per * world, dtype=t.dtype, device=t.device)
-    padded[:n] = flat
-    recv = torch.empty_like(padded)
+    padded, recv, mine, gathered = _exchange_buffers(n, t.dtype, t.device, world)
+    per = mine.numel()
+    padded[:n].copy_(flat)
     dist.all_to_all_single(recv, padded, group=group)  # recv[r*per:(r+1)*per] = rank r's copy of my slice
     parts = recv.view(world, per)
-    mine = parts[0].clone()
+    mine.copy_(parts[0])
     for r in range(1, world):
         mine += parts[r]
-    gathered = torch.empty_like(padded)
     if hasattr(dist, "all_gather_into_tensor") and t.is_cuda:
         dist.all_gather_into_tensor(gathered, mine, group=group)
     else:
-        chunks = list(gathered.view(world, per).unbind(0))
-        dist.all_gather(chunks, mine, group=group)
-        gathered = torch.cat(chunks)
+        dist.all_gather(list(gathered.view(world, per).unbind(0)), mine, group=group)
     flat.copy_(gathered[:n])
     return t
 
 
-def sharded_iteration(nviews: int, forward: Callable[[int, int], None],
-                      backward: Callable[[int, int, torch.Tensor], None],
-                      update: Callable[[torch.Tensor], None], ht: torch.Tensor, group=None) -> None:
-    """One MLEM iteration with views split over the ranks of `group`.
-
-    forward(first, count): ratios of the local views; backward(first, count,
-    ht): partial back projection into ht (overwrite); update(ht): the
-    multiplicative update with the summed ht."""
+def sharded_mlem_iteration(P, g, f, ht, group=None) -> None:
+    """One MLEM iteration of plan P with its views split over the ranks of
+    `group`: P.mlem_forward / mlem_backward over this rank's views (the C ABI's
+    recon_mlem_forward / recon_mlem_backward), the rank-ordered sum of the
+    partial images, then P.mlem_update (recon_mlem_update) on every rank.  P is
+    any object with those three methods and `nproj`."""
     rank = dist.get_rank(group) if dist.is_initialized() else 0
     world = dist.get_world_size(group) if dist.is_initialized() else 1
-    first, count = view_range(nviews, rank, world)
-    forward(first, count)
-    backward(first, count, ht)
+    first, count = view_range(P.nproj, rank, world)
+    P.mlem_forward(g, f, first, count)
+    P.mlem_backward(ht, first, count)
     if world > 1:
         ordered_sum_(ht, group)
-    update(ht)
+    P.mlem_update(f, ht)

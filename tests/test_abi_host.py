@@ -140,7 +140,7 @@ def test_plan_rejects_bad_geometry():
     assert lib.recon_plan_create(C.byref(geometry(small_cfg(Rf=10.0))), C.byref(o), C.byref(h)) == 2
     o.arith = 7
     assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1
-    o.arith, o.siddon_bp = 0, 3
+    o.arith, o.siddon_bp = 0, 4  # 0..3 are AUTO, GATHER, RAY, TUNED
     assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1
 
 

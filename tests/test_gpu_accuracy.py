@@ -40,10 +40,10 @@ if not torch.cuda.is_available():
     pytest.skip("no CUDA device", allow_module_level=True)
 
 from oracle import oracle as O  # noqa: E402
-from recon_b200 import (ARITH_COMPAT, PROJECTOR_BACK, PROJECTOR_FORWARD, SIDDON_BP_GATHER, SIDDON_BP_RAY,  # noqa: E402
-                        Options, Plan, mlem_from_cfg)
+from recon_b200 import (ARITH_COMPAT, FP_COLUMNS, PROJECTOR_BACK, PROJECTOR_FORWARD, SIDDON_BP_GATHER,  # noqa: E402
+                        SIDDON_BP_RAY, Options, Plan, mlem_from_cfg)
 from recon_b200.configs import CPU_SMALL, PLAIN_GPU, geom_dict, scaled  # noqa: E402
-from recon_b200.phantom import noisy, phantom  # noqa: E402
+from recon_b200.phantom import noisy, phantom, workload  # noqa: E402
 
 COUNT_GEOMS = {
     "plain": small_cfg(),
@@ -61,6 +61,8 @@ COUNT_GEOMS = {
 def test_pair_counts_equal(name, design):
     cfg = COUNT_GEOMS[name]
     P = Plan(cfg, Options(siddon_bp=SIDDON_BP_GATHER if design == "gather" else SIDDON_BP_RAY))
+    # mirror pairing wherever the z table is symmetric: no Dz, an even slice count
+    assert P.mirror_pairs == (cfg["Dz"] == 0.0 and int(cfg["Zdim"]) % 2 == 0)
     walk = P.count_intersections()
     assert walk > 0
     assert P.count_projector_pairs(PROJECTOR_FORWARD) == walk
@@ -93,10 +95,12 @@ def test_plain_gpu_workload_accuracy_and_counts():
     cfg = dict(PLAIN_GPU)
     nproj = int(cfg["NumProj"])
     dang = np.float32(cfg["DeltaAng"])
-    vol = phantom(cfg, device=torch.device("cuda"))
-    P = Plan(cfg)
-    g = noisy(P.fp_views(vol), cfg["I0"], cfg["seed"])
+    vol, g = workload(cfg, "cuda")  # the benchmark's own inputs
     del vol
+    P = Plan(cfg)
+    # the benchmarked designs: detector-column forward projector, gather back
+    # projector, both on mirrored row / voxel pairs
+    assert P.forward_projector == FP_COLUMNS and P.siddon_bp == SIDDON_BP_GATHER and P.mirror_pairs
     walk = P.count_intersections()
     pairs = {"walk": walk, "forward": P.count_projector_pairs(PROJECTOR_FORWARD),
              "back": P.count_projector_pairs(PROJECTOR_BACK)}

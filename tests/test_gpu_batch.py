@@ -99,3 +99,27 @@ def test_batch_rejects_unsupported_and_mismatched():
         B.mlem(gs[:1], 1)
     with pytest.raises(ValueError):
         B.mlem([gs[1], gs[0]], 1)
+
+
+def test_tuned_back_projector_same_choice_and_bits():
+    # SIDDON_BP_TUNED measures both back projectors on each geometry at plan
+    # creation and keeps the faster, remembered per geometry: the batch's plans
+    # and later plain plans of the same geometries choose alike and agree bit for bit
+    from recon_b200 import SIDDON_BP_GATHER, SIDDON_BP_RAY, SIDDON_BP_TUNED
+
+    opt = Options(siddon_bp=SIDDON_BP_TUNED)
+    gs = _sinos(MIXED, 12)
+    fs = Batch(MIXED, opt).mlem(gs, 2)
+    torch.cuda.synchronize()
+    for p, (c, g) in enumerate(zip(MIXED, gs)):
+        P = Plan(c, opt)
+        assert P.siddon_bp in (SIDDON_BP_GATHER, SIDDON_BP_RAY)
+        assert Plan(c, opt).siddon_bp == P.siddon_bp
+        assert np.array_equal(_bits(fs[p]), _bits(P.mlem(g, 2))), p
+    # and the tuned plan is the EXACT projector pair: against FP64
+    c = MIXED[0]
+    geo = O.Geom.from_dict(geom_dict(c))
+    y = np.random.default_rng(3).random(int(c["NumProj"]) * geo.npix).astype(np.float32)
+    bp = Plan(c, opt).bp_views(torch.from_numpy(y).cuda().reshape(int(c["NumProj"]), -1, int(c["AxPixels"])))
+    ref = O.x_bp_all(geo, int(c["NumProj"]), np.float32(c["DeltaAng"]), y.astype(np.float64))
+    assert rel_l2(bp.cpu().numpy().ravel(), ref) < 1e-5

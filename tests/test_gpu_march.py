@@ -1,5 +1,11 @@
-"""Ray-marching forward projection (recon_march_fp_view) against its FP64 oracle.
+"""Ray-marching forward projection (recon_march_fp_view).
 
+REFERENCE mode against the reference's own kernel: forward_projection
+(CT_Recon/hf_cuda_kernels.cuh:126-180), built for sm_100a from its sources
+(oracle/_ref/libref_gpu.so) with its 3D texture replaced by a point-sampled,
+border-addressed stand-in over normalised coordinates (oracle/ref_shim/common/
+ref_prelude_gpu.h), launched once per depth plane: bit-identical images.
+Both modes against the FP64 restatement (orc_m_fp_view):
 GEOMETRIC: trilinear plane samples; FP32 against FP64, rel. L2 <= 1e-5.
 REFERENCE: point samples of normalised coordinates; a sample whose coordinate
 lies within FP32 rounding of a texel boundary may take the neighbouring texel,
@@ -56,3 +62,23 @@ def test_march_rejects_bad_arguments():
         P.march_fp_view(vol, 0.0, 7)
     with pytest.raises(Exception):
         P.march_fp_view(vol, float("nan"), VOXEL_GEOMETRIC)
+
+
+REFG = O.ref_gpu()
+
+
+@pytest.mark.skipif(REFG is None or not hasattr(REFG, "ref_gpu_march_fp_view"),
+                    reason="reference sm_100a build missing")
+@pytest.mark.parametrize("name", list(GEOMS))
+def test_reference_mode_vs_reference_kernel(name):
+    cfg, opts = GEOMS[name]
+    P = Plan(cfg, opts)
+    g = O.Geom.from_dict(geom_dict(cfg))
+    vol = np.random.default_rng(43).random(g.nvox).astype(np.float32)
+    dvol = torch.from_numpy(vol).cuda().reshape(P.shape_vol)
+    for ang in (0.0, 37.5, 90.0, 211.25, 359.0):
+        out = P.march_fp_view(dvol, ang, VOXEL_REFERENCE).cpu().numpy().ravel()
+        ref = np.zeros(g.npix, np.float32)
+        REFG.ref_gpu_march_fp_view(g, ang, vol, ref)
+        assert np.any(ref != 0), ang
+        assert np.array_equal(out.view(np.uint32), ref.view(np.uint32)), (ang, rel_l2(out, ref))

@@ -4,7 +4,7 @@ analytic known answers.  No GPU needed.
 The reference ships no tests, fixtures or golden vectors, so the FP32
 restatement (oracle/siddon_oracle.c) is pinned by running the reference's
 kernel sources themselves, compiled for the host (oracle/_ref/libref_cpu.so,
-built from /root/reference by oracle/build_oracle.py): set-up arrays,
+built from the reference's sources by oracle/build_oracle.py): set-up arrays,
 per-step traces, projections, back projections and MLEM must agree bit for bit.
 The FP64 oracle is pinned by analytic intersection lengths.
 """

@@ -1,6 +1,11 @@
-"""View-sharded MLEM with world_size 2 over gloo on CPU: the sharded iteration
-equals the single-process one (FP64 oracle as the per-rank projector), the
-cross-rank sum is taken in rank order, and every rank ends with the same bits."""
+"""View-sharded MLEM with world_size 2 over gloo on CPU.
+
+recon_b200.sharding.sharded_mlem_iteration -- the function bench.py runs at
+N > 1 -- drives a CPU stand-in of the plan with the same three methods
+(mlem_forward / mlem_backward / mlem_update over a view range, backed by the
+FP64 oracle).  The sharded iteration equals the single-process one, the
+cross-rank sum is taken in rank order, and every rank ends with the same
+bits."""
 import os
 import tempfile
 
@@ -47,37 +52,50 @@ def _projector(O, g, nproj, dang):
     return fp, bp
 
 
+class _OraclePlan:
+    """The split-iteration methods of recon_b200.Plan (recon_mlem_forward,
+    recon_mlem_backward, recon_mlem_update), restated on the FP64 oracle: the
+    ratios of views [first, first + count) kept inside, their back projection
+    into ht, and f = (sens != 0) ? f * ht / sens : 0."""
+
+    def __init__(self, O, g, nproj, dang):
+        self.nproj = nproj
+        self.fp, self.bp = _projector(O, g, nproj, dang)
+        self.npix = g.npix
+        self.sens = O.x_bp_all(g, nproj, dang, np.ones(nproj * g.npix), threads=1)
+        self.ratio = None
+
+    def mlem_forward(self, g, f, first, count):
+        hf = self.fp(f.numpy(), first, count)
+        gm = g.numpy()[first * self.npix:(first + count) * self.npix]
+        self.ratio = np.where(hf != 0, gm / np.where(hf != 0, hf, 1), 0.0)
+
+    def mlem_backward(self, ht, first, count):
+        ht.copy_(torch.from_numpy(self.bp(self.ratio, first, count)))
+
+    def mlem_update(self, f, ht):
+        fv, h, s = f.numpy(), ht.numpy(), self.sens
+        fv[:] = np.where(s != 0, fv * h / np.where(s != 0, s, 1), 0.0)
+
+
 def _worker(rank, world, init_file, out_dir):
     dist.init_process_group("gloo", init_method=f"file://{init_file}", rank=rank, world_size=world)
-    from recon_b200.sharding import ordered_sum_, sharded_iteration, view_range
+    from recon_b200.sharding import ordered_sum_, sharded_mlem_iteration, view_range
 
     O, cfg, g, meas = _setup()
     nproj, dang = 10, np.float32(36.0)
-    fp, bp = _projector(O, g, nproj, dang)
-    sens = O.x_bp_all(g, nproj, dang, np.ones(nproj * g.npix), threads=1)
-    f = np.ones(g.nvox)
-    state = {}
-
-    def forward(first, count):
-        hf = fp(f, first, count)
-        gm = meas[first * g.npix:(first + count) * g.npix]
-        state["ratio"] = np.where(hf != 0, gm / np.where(hf != 0, hf, 1), 0.0)
-
-    def backward(first, count, ht):
-        ht.copy_(torch.from_numpy(bp(state["ratio"], first, count)))
-
-    def update(ht):
-        h = ht.numpy()
-        f[:] = np.where(sens != 0, f * h / np.where(sens != 0, sens, 1), 0.0)
-
+    P = _OraclePlan(O, g, nproj, dang)
+    f = torch.ones(g.nvox, dtype=torch.float64)
+    gt = torch.from_numpy(meas)
     ht = torch.zeros(g.nvox, dtype=torch.float64)
     for _ in range(2):
-        sharded_iteration(nproj, forward, backward, update, ht)
-    np.save(os.path.join(out_dir, f"f{rank}.npy"), f)
-    # the rank-ordered sum itself
-    x = torch.full((7,), float(rank + 1), dtype=torch.float64) * torch.arange(7, dtype=torch.float64)
-    ordered_sum_(x)
-    np.save(os.path.join(out_dir, f"s{rank}.npy"), x.numpy())
+        sharded_mlem_iteration(P, gt, f, ht)
+    np.save(os.path.join(out_dir, f"f{rank}.npy"), f.numpy())
+    # the rank-ordered sum itself, twice (its exchange buffers are reused)
+    for rep in range(2):
+        x = torch.full((7,), float(rank + 1), dtype=torch.float64) * torch.arange(7, dtype=torch.float64)
+        ordered_sum_(x)
+        np.save(os.path.join(out_dir, f"s{rank}_{rep}.npy"), x.numpy())
     assert view_range(10, rank, world)[1] == 5
     dist.barrier()
     dist.destroy_process_group()
@@ -90,8 +108,10 @@ def test_sharded_mlem_two_ranks():
     f0 = np.load(os.path.join(out_dir, "f0.npy"))
     f1 = np.load(os.path.join(out_dir, "f1.npy"))
     assert np.array_equal(f0, f1)
-    s = np.load(os.path.join(out_dir, "s0.npy"))
-    assert np.array_equal(s, 3.0 * np.arange(7)) and np.array_equal(s, np.load(os.path.join(out_dir, "s1.npy")))
+    for rep in range(2):
+        s = np.load(os.path.join(out_dir, f"s0_{rep}.npy"))
+        assert np.array_equal(s, 3.0 * np.arange(7))
+        assert np.array_equal(s, np.load(os.path.join(out_dir, f"s1_{rep}.npy")))
     # single-process reference
     O, cfg, g, meas = _setup()
     nproj, dang = 10, np.float32(36.0)
