@@ -50,6 +50,7 @@ def parse_args():
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched-vs-plain leg and print it as the JSON line")
     ap.add_argument("--no-voxel", action="store_true", help="skip the voxel-driven back projector leg")
+    ap.add_argument("--no-compat", action="store_true", help="skip the COMPAT (reference arithmetic) leg")
     ap.add_argument("--batched-problems", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=20)
     return ap.parse_args()
@@ -301,6 +302,35 @@ def voxel_leg(cfg, g, steps: int, warmup: int, device_index: int):
     ms = a.elapsed_time(b) / steps
     return {"value": 1e3 / ms, "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
             "back_projector": "voxel-driven, FP32 bilinear taps gathered per voxel column (geometric mode)"}
+
+
+def compat_leg(cfg, g, device_index: int, budget_s: float = 10.0):
+    """The drop-in default path on the same workload: COMPAT arithmetic (the
+    reference's FP32 Siddon traversal, hf_siddon_class.hpp:44-47 defaults),
+    one thread per ray, int64 fixed-point scatter per view.  One untimed
+    iteration, then iterations timed one by one with CUDA events until
+    `budget_s` of timed work or 5 iterations."""
+    import torch
+
+    from recon_b200 import ARITH_COMPAT, Options, Plan
+
+    P = Plan(cfg, Options(arith=ARITH_COMPAT, device=device_index))
+    P.mlem_prepare()
+    f = P.new_volume(1.0)
+    P.mlem_iteration(g, f)
+    times = []
+    while len(times) < 5 and sum(times) < budget_s * 1e3:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        P.mlem_iteration(g, f)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = sum(times) / len(times)
+    P.close()
+    return {"value": 1e3 / ms, "unit": UNIT, "ms_per_step": ms, "steps": len(times), "warmup": 1,
+            "arithmetic": "COMPAT (the reference's FP32 traversal; bit-exact per ray)"}
 
 
 def ref_view_seconds(R, O, geo, cfg, view, steps, f, gview, ht):
@@ -679,6 +709,9 @@ def main():
         del P
         torch.cuda.empty_cache()
         out["voxel_bp"] = voxel_leg(cfg, g, max(3, args.steps // 4), args.warmup, local)
+    if world == 1 and not args.no_compat and args.sino == "f32":
+        torch.cuda.empty_cache()
+        out["compat"] = compat_leg(cfg, g, local)
     if not args.no_batched:
         del g_host, f_host, g, vol
         torch.cuda.empty_cache()

@@ -195,7 +195,56 @@ constexpr int kGatherTileX = 4;
 struct GatherConst {
     float eu, ou;  // detector column of a point (a, b) of the view frame: a / (b + Rf) * eu + ou
     float ez, oz;  // detector row of height z at depth d (t = d - Rf):      z / d * ez + oz
+    int vec4;      // X % 4 == 0 and the volume, sensitivity 16-byte aligned: float4 epilogue
 };
+
+// MLEM update of one voxel, as update_kernel computes it
+__device__ __forceinline__ float gather_update(float f, float ht, float sens)
+{
+    return (sens != 0.0f) ? __fdiv_rn(__fmul_rn(f, ht), sens) : 0.0f;
+}
+
+// The CTA's epilogue for one chunk of planes, coalesced along x.  Warp
+// w = xl + kGatherTileX * yl (column i0 + xl, j0 + yl) has left its sum for
+// entry e in stage[w * NE + e]; entry e belongs to plane zplane(e), or to none
+// when that is negative.  EPI 0 writes the sums, EPI 1 the updated image.  With
+// C.vec4 a thread moves the tile's four x-neighbours of one (plane, row) as one
+// float4, otherwise one voxel, the CTA's threads walking (x, y, entry) x fastest.
+template <int EPI, int NE, class ZPlane>
+__device__ __forceinline__ void gather_tile_epilogue(const ExactGeom& G, bool vec4, const float* stage, int i0,
+                                                     int j0, ZPlane zplane, float* __restrict__ vol,
+                                                     const float* __restrict__ sens)
+{
+    constexpr int tx = kGatherTileX, ty = kGatherWarps / kGatherTileX;
+    static_assert(tx == 4, "the float4 epilogue moves four x-neighbours");
+    const size_t plane = (size_t)G.X * G.Y;
+    if (vec4) {
+        for (int q = threadIdx.x; q < NE * ty; q += blockDim.x) {
+            const int yl = q % ty, e = q / ty;
+            const int k = zplane(e), j = j0 + yl;
+            if (k < 0 || j >= G.Y) continue;
+            const size_t v = (size_t)k * plane + (size_t)j * G.X + (size_t)i0;
+            const float* h = stage + yl * tx * NE + e;
+            float4 o = make_float4(h[0], h[NE], h[2 * NE], h[3 * NE]);
+            if (EPI == 1) {
+                const float4 f = *reinterpret_cast<const float4*>(vol + v);
+                const float4 sv = *reinterpret_cast<const float4*>(sens + v);
+                o = make_float4(gather_update(f.x, o.x, sv.x), gather_update(f.y, o.y, sv.y),
+                                gather_update(f.z, o.z, sv.z), gather_update(f.w, o.w, sv.w));
+            }
+            *reinterpret_cast<float4*>(vol + v) = o;
+        }
+    } else {
+        for (int q = threadIdx.x; q < NE * ty * tx; q += blockDim.x) {
+            const int xl = q % tx, yl = (q / tx) % ty, e = q / (tx * ty);
+            const int k = zplane(e), i = i0 + xl, j = j0 + yl;
+            if (k < 0 || i >= G.X || j >= G.Y) continue;
+            const size_t v = (size_t)k * plane + (size_t)j * G.X + (size_t)i;
+            const float h = stage[(yl * tx + xl) * NE + e];
+            vol[v] = (EPI == 1) ? gather_update(vol[v], h, sens[v]) : h;
+        }
+    }
+}
 
 // A warp's column seen from one view: detector columns u_lo..u_hi and, for the
 // first two (sl = 0, 1), the column's piece [A, B] of their rays, the row
@@ -283,14 +332,14 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * kGatherTileX + warp % kGatherTileX;
-    const int j = blockIdx.y * (kGatherWarps / kGatherTileX) + warp / kGatherTileX;
-    if (i >= G.X || j >= G.Y) return;  // whole warps; no block barrier follows
+    const int i0 = blockIdx.x * kGatherTileX, j0 = blockIdx.y * (kGatherWarps / kGatherTileX);
+    const int i = i0 + warp % kGatherTileX, j = j0 + warp / kGatherTileX;
+    // a warp past the volume's edge takes no view but joins the epilogue's barriers
+    const unsigned nview_w = (i < G.X && j < G.Y) ? nview : 0u;
     GatherView* sv = sview[warp];
     float* acc2 = sacc2[warp];
     const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
     const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
-    const size_t plane = (size_t)G.X * G.Y;
     // candidate rows are widened by 0.002 row on either side: about ten times the
     // FP32 error of the row bounds (values of a few hundred rows, a few roundings),
     // small enough that a voxel rarely shows a second candidate that is not one
@@ -402,8 +451,8 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
                     }
                 }
             };
-            for (unsigned vb = 0; vb < nview; vb += 32) {
-                const unsigned nb = min(32u, nview - vb);
+            for (unsigned vb = 0; vb < nview_w; vb += 32) {
+                const unsigned nb = min(32u, nview_w - vb);
                 if ((unsigned)lane < nb)  // lane q sets up view vb + q
                     sv[lane] = gather_view(G, C, txy, kxy, cs, view0 + vb + lane, i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo,
                                            dz32);
@@ -456,18 +505,14 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_kernel(
             for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
             if (lane == 0 && c) atomicAdd(npairs, c);
         } else {
+            // the sums into the staging entries (each lane its own), then the
+            // CTA's coalesced epilogue
 #pragma unroll
-            for (int s = 0; s < SLOTS; ++s) {
-                if (s >= nslot) continue;
-                const size_t vox = (size_t)i + (size_t)j * G.X + (size_t)(k0 + lane + 32 * s) * plane;
-                const float ht = acc[s] + acc2[s * 32 + lane];
-                if (EPI == 1) {
-                    const float svv = sens[vox];
-                    vol[vox] = (svv != 0.0f) ? __fdiv_rn(__fmul_rn(vol[vox], ht), svv) : 0.0f;
-                } else {
-                    vol[vox] = ht;
-                }
-            }
+            for (int s = 0; s < SLOTS; ++s) acc2[s * 32 + lane] += acc[s];
+            __syncthreads();
+            gather_tile_epilogue<EPI, SLOTS * 32>(
+                G, C.vec4 != 0, &sacc2[0][0], i0, j0, [&](int e) { return k0 + e < G.Z ? k0 + e : -1; }, vol, sens);
+            __syncthreads();  // the next chunk clears the entries
         }
     }
 }
@@ -501,15 +546,14 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_mirror_kernel(
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * kGatherTileX + warp % kGatherTileX;
-    const int j = blockIdx.y * (kGatherWarps / kGatherTileX) + warp / kGatherTileX;
-    if (i >= G.X || j >= G.Y) return;  // whole warps; no block barrier follows
+    const int i0 = blockIdx.x * kGatherTileX, j0 = blockIdx.y * (kGatherWarps / kGatherTileX);
+    const int i = i0 + warp % kGatherTileX, j = j0 + warp / kGatherTileX;
+    const unsigned nview_w = (i < G.X && j < G.Y) ? nview : 0u;  // as in bp_gather_kernel
     GatherView* sv = sview[warp];
     float* acc2 = sacc2[warp][0];
     float* acc2m = sacc2[warp][1];
     const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
     const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
-    const size_t plane = (size_t)G.X * G.Y;
     const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;  // margins as in bp_gather_kernel
     const float dz32 = 32.0f * G.vox[2];
     const int Zh = G.Z / 2;
@@ -611,8 +655,8 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_mirror_kernel(
                 }
             }
         };
-        for (unsigned vb = 0; vb < nview; vb += 32) {
-            const unsigned nb = min(32u, nview - vb);
+        for (unsigned vb = 0; vb < nview_w; vb += 32) {
+            const unsigned nb = min(32u, nview_w - vb);
             if ((unsigned)lane < nb)  // lane q sets up view vb + q
                 sv[lane] = gather_view(G, C, txy, kxy, cs, view0 + vb + lane, i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo,
                                        dz32);
@@ -657,23 +701,21 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_mirror_kernel(
             for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
             if (lane == 0 && c) atomicAdd(npairs, c);
         } else {
+            // entries [0, 32 PS) the lower voxels k0 + e, [32 PS, 64 PS) their mirrors
 #pragma unroll
             for (int s = 0; s < PS; ++s) {
-                if (s >= nslot) continue;
-                const int k = k0 + lane + 32 * s;
-                const size_t col0 = (size_t)i + (size_t)j * G.X;
-                const size_t v0 = col0 + (size_t)k * plane, v1 = col0 + (size_t)(G.Z - 1 - k) * plane;
-                const float h0 = acc[s] + acc2[s * 32 + lane], h1 = accm[s] + acc2m[s * 32 + lane];
-                if (EPI == 1) {
-                    const float s0 = sens[v0], s1 = sens[v1];
-                    const float f0 = vol[v0], f1 = vol[v1];
-                    vol[v0] = (s0 != 0.0f) ? __fdiv_rn(__fmul_rn(f0, h0), s0) : 0.0f;
-                    vol[v1] = (s1 != 0.0f) ? __fdiv_rn(__fmul_rn(f1, h1), s1) : 0.0f;
-                } else {
-                    vol[v0] = h0;
-                    vol[v1] = h1;
-                }
+                acc2[s * 32 + lane] += acc[s];
+                acc2m[s * 32 + lane] += accm[s];
             }
+            __syncthreads();
+            gather_tile_epilogue<EPI, 64 * PS>(
+                G, C.vec4 != 0, &sacc2[0][0][0], i0, j0,
+                [&](int e) {
+                    const int k = k0 + (e < 32 * PS ? e : e - 32 * PS);
+                    return k >= Zh ? -1 : (e < 32 * PS ? k : G.Z - 1 - k);
+                },
+                vol, sens);
+            __syncthreads();  // the next chunk clears the entries
         }
     }
 }
@@ -1408,6 +1450,8 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
     C.ou = (float)(-((double)E.Dx + E.ud0) / E.du);
     C.ez = (float)((double)E.Ry / E.dv);
     C.oz = (float)(-((double)E.Dz + E.vd0) / E.dv);
+    C.vec4 = (E.X % 4 == 0) && (reinterpret_cast<uintptr_t>(vol) % 16 == 0) &&
+             (reinterpret_cast<uintptr_t>(sens) % 16 == 0);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
     auto kernel = [] {
         if constexpr (MIRROR) return exact::bp_gather_mirror_kernel<EPI, ST, SLOTS>;

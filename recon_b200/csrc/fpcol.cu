@@ -22,8 +22,9 @@
 // from the plane values plane_t of the ray walk (exact_device.cuh) and of both
 // back projectors, so the projector pair stays an exact transpose; only the
 // order of the ray sum's additions differs from the walk.  Ray sums are
-// compensated (Kahan) over blocks of 8 pieces: each block's 16 products are
-// summed in FP32 and the block sums Kahan-added.
+// compensated (Kahan) over blocks of pieces (8 per block, 16 in the mirrored
+// walk): each block's products are summed in FP32 and the block sums
+// Kahan-added.
 #include "exact_device.cuh"
 #include "internal.h"
 
@@ -210,14 +211,14 @@ template <bool KAHAN, bool FAST, bool COUNT>
 __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ volz, const float2* spc, int jb, int je,
                                                    float cur, int kaddr, float kf, float tzn, float S, float O, int Z)
 {
-    const int zp1 = Z + 1;
+    int dm = Z + 1 - 2 * kaddr;  // the mirror row's offset from row v's in the same column
     float acc = 0.0f, comp = 0.0f, accm = 0.0f, compm = 0.0f, f1 = 0.0f, f1m = 0.0f;
     auto piece = [&](int j, float& blk, float& blkm) {
         const float2 pc = spc[j];
         const float B = pc.x;
         const int cb = __float_as_int(pc.y);
         const float* p = volz + (cb + kaddr);
-        const float* pm = volz + (cb + (zp1 - kaddr));
+        const float* pm = p + dm;
         const bool cross = tzn < B;
         const float m = fminf(tzn, B);
         if (COUNT) {  // layers 0 .. Z-1 sit at kaddr 1 .. Z, for both rows
@@ -239,6 +240,7 @@ __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ vol
         }
         if (cross) {
             kaddr -= 1;
+            dm += 2;
             kf -= 1.0f;
             tzn = fmaf(kf, S, O);
             if (!FAST && kaddr == 0) tzn = __int_as_float(0x7f800000);  // left through the bottom
@@ -246,10 +248,11 @@ __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ vol
         cur = B;
     };
     int j = jb;
-    for (; j + 7 <= je; j += 8) {
+    // blocks of 16 pieces: the pair's loads of a block issue together
+    for (; j + 15 <= je; j += 16) {
         float blk = 0.0f, blkm = 0.0f;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) piece(j + q, blk, blkm);
+        for (int q = 0; q < 16; ++q) piece(j + q, blk, blkm);
         if (KAHAN && !COUNT) {
             kahan_add(acc, comp, blk);
             kahan_add(accm, compm, blkm);
