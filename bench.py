@@ -388,6 +388,10 @@ def reference_gpu_leg(O, geo, cfg, vol, gviews: dict) -> dict | None:
     R = O.ref_gpu()
     if R is None:
         return None
+    import torch
+
+    if not torch.cuda.is_available():  # the reference exits the process on a CUDA error
+        return {"unavailable": "no CUDA device"}
     n = int(cfg["NumProj"])
     dang = np.float32(cfg["DeltaAng"])
     vol32 = vol.astype(np.float32)

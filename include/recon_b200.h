@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define RECON_B200_ABI_VERSION 2
+#define RECON_B200_ABI_VERSION 3
 
 typedef enum {
     RECON_OK = 0,
@@ -143,6 +143,13 @@ typedef struct {
     int voxel_mode; /* recon_voxel_mode_t, default GEOMETRIC */
     int device;     /* CUDA device ordinal, default 0 */
     int siddon_bp;  /* recon_siddon_bp_t, default AUTO (EXACT arithmetic only) */
+    int fp_block;   /* detector-column forward projector over xy blocks of
+                     * fp_block x fp_block voxel columns, one block at a time
+                     * (at most 64 blocks): 0 = AUTO (blocks where the volume's
+                     * z-fastest copy exceeds 96 MiB, each block's share at most
+                     * 40 MiB, so the views in flight reuse it from L2), -1 =
+                     * never, n > 0 = n.  Same lengths; the ray sums add the
+                     * blocks' shares in block order. */
 } recon_options_t;
 
 typedef struct recon_plan* recon_plan_t;
@@ -188,6 +195,7 @@ recon_status_t recon_plan_siddon_bp(recon_plan_t plan, int* design);
  * one forward projector. */
 #define RECON_FP_RAY_WALK 0
 #define RECON_FP_COLUMNS 1
+#define RECON_FP_COLUMN_BLOCKS 2 /* detector columns, volume walked in xy blocks (fp_block) */
 recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design);
 /* *paired = 1 when the plan's EXACT projectors take detector rows (and, in
  * the gather back projector, voxels) in pairs mirrored about the source plane

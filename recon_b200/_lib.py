@@ -29,7 +29,8 @@ PROJECTOR_FORWARD = 0  # RECON_PROJECTOR_FORWARD
 PROJECTOR_BACK = 1  # RECON_PROJECTOR_BACK
 FP_RAY_WALK = 0  # RECON_FP_RAY_WALK
 FP_COLUMNS = 1  # RECON_FP_COLUMNS
-ABI_VERSION = 2  # RECON_B200_ABI_VERSION: the layout of the structures above
+FP_COLUMN_BLOCKS = 2  # RECON_FP_COLUMN_BLOCKS
+ABI_VERSION = 3  # RECON_B200_ABI_VERSION: the layout of the structures above
 
 
 class ReconError(RuntimeError):
@@ -71,7 +72,7 @@ class FilePaths(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("arith", C.c_int), ("sum", C.c_int), ("sino", C.c_int), ("bp", C.c_int),
-                ("voxel_mode", C.c_int), ("device", C.c_int), ("siddon_bp", C.c_int)]
+                ("voxel_mode", C.c_int), ("device", C.c_int), ("siddon_bp", C.c_int), ("fp_block", C.c_int)]
 
 
 _lib = None

@@ -27,9 +27,11 @@ class Options:
     voxel_mode: int = L.VOXEL_GEOMETRIC
     device: int = 0
     siddon_bp: int = L.SIDDON_BP_AUTO
+    fp_block: int = 0
 
     def c(self) -> L.Options:
-        return L.Options(self.arith, self.sum, self.sino, self.bp, self.voxel_mode, self.device, self.siddon_bp)
+        return L.Options(self.arith, self.sum, self.sino, self.bp, self.voxel_mode, self.device, self.siddon_bp,
+                         self.fp_block)
 
 
 def geometry(cfg: dict) -> L.Geometry:

@@ -74,6 +74,9 @@ static recon_status_t validate(const recon_geometry_t& g, const recon_options_t&
     if (o.siddon_bp != RECON_SIDDON_BP_AUTO && o.siddon_bp != RECON_SIDDON_BP_GATHER &&
         o.siddon_bp != RECON_SIDDON_BP_RAY && o.siddon_bp != RECON_SIDDON_BP_TUNED)
         return fail(RECON_ERR_INVALID_ARGUMENT, "unknown siddon_bp option");
+    if (o.fp_block < -1) return fail(RECON_ERR_INVALID_ARGUMENT, "fp_block must be -1, 0 or a block side");
+    if (o.fp_block > 0 && ((v.Xdim + o.fp_block - 1) / o.fp_block) * ((v.Ydim + o.fp_block - 1) / o.fp_block) > 64)
+        return fail(RECON_ERR_INVALID_ARGUMENT, "fp_block: more than 64 xy blocks");
     if (o.arith == RECON_ARITH_EXACT) {
         if (c.xangle != 0.0f || c.yangle != 0.0f || c.zangle != 0.0f)
             return fail(RECON_ERR_UNSUPPORTED,
@@ -233,6 +236,7 @@ recon_status_t recon_default_options(recon_options_t* opt)
     opt->voxel_mode = RECON_VOXEL_GEOMETRIC;
     opt->device = 0;
     opt->siddon_bp = RECON_SIDDON_BP_AUTO;
+    opt->fp_block = 0;
     return RECON_OK;
 }
 
@@ -337,7 +341,7 @@ recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design)
     if (!plan || !design) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
     if (plan->opt.arith != RECON_ARITH_EXACT)
         return fail(RECON_ERR_UNSUPPORTED, "COMPAT plans have a single forward projector");
-    *design = plan->fp_column ? RECON_FP_COLUMNS : RECON_FP_RAY_WALK;
+    *design = !plan->fp_column ? RECON_FP_RAY_WALK : plan->col_block > 0 ? RECON_FP_COLUMN_BLOCKS : RECON_FP_COLUMNS;
     return RECON_OK;
 }
 

@@ -16,27 +16,34 @@ namespace exact {
 
 __device__ __forceinline__ float plane_t(int k, float S, float O, int kc) { return fmaf((float)(k - kc), S, O); }
 
-// Voxel i along an axis with N voxels: the voxel whose t-interval [lo, hi)
-// contains t (entry: lo <= t < hi) or (lo, hi] (exit: lo < t <= hi), found
-// from an FP64 estimate and corrected against the FP32 plane values.
+// Voxel i in [lo, hi) along an axis: the voxel whose t-interval [t_i, t_i+1)
+// contains t (entry: t_i <= t < t_i+1) or (t_i, t_i+1] (exit), ends ordered,
+// found from an FP64 estimate and corrected against the FP32 plane values.
 template <bool ENTRY>
-__device__ __forceinline__ int locate(float t, float S, float O, int kc, int N, double invS)
+__device__ __forceinline__ int locate_in(float t, float S, float O, int kc, int lo, int hi, double invS)
 {
     double kf = (double)kc + ((double)t - (double)O) * invS;
-    int i = (int)floor(fmin(fmax(kf, -1.0), (double)N));
-    i = min(max(i, 0), N - 1);
+    int i = (int)floor(fmin(fmax(kf, (double)lo - 1.0), (double)hi));
+    i = min(max(i, lo), hi - 1);
     const int up = (S > 0.0f) ? 1 : -1;  // index step toward larger t
 #pragma unroll 1
     for (int it = 0; it < 6; ++it) {
         float t0 = plane_t(i, S, O, kc), t1 = plane_t(i + 1, S, O, kc);
-        float lo = fminf(t0, t1), hi = fmaxf(t0, t1);
-        bool before = ENTRY ? (t < lo) : (t <= lo);
-        bool after = ENTRY ? (t >= hi) : (t > hi);
+        float a = fminf(t0, t1), b = fmaxf(t0, t1);
+        bool before = ENTRY ? (t < a) : (t <= a);
+        bool after = ENTRY ? (t >= b) : (t > b);
         int ni = before ? i - up : (after ? i + up : i);
-        if (ni == i || ni < 0 || ni >= N) break;
+        if (ni == i || ni < lo || ni >= hi) break;
         i = ni;
     }
     return i;
+}
+
+// The same over the whole axis of N voxels.
+template <bool ENTRY>
+__device__ __forceinline__ int locate(float t, float S, float O, int kc, int N, double invS)
+{
+    return locate_in<ENTRY>(t, S, O, kc, 0, N, invS);
 }
 
 template <class T>

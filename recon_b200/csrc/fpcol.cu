@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 namespace rb {
 namespace exact {
@@ -323,7 +324,12 @@ __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, cons
 // MODE 0: out = projection (w * sum); MODE 1 (MLEM): out = w * g / Hf (0 where
 // Hf == 0), the Siddon back projector's input; MODE 2: out = g / Hf (the
 // voxel-driven back projector's); MODE 3: the (ray, voxel) pairs of positive
-// length are counted into out[0] (OT = unsigned long long).  g is read [view][v][u]; out is written in
+// length are counted into out[0] (OT = unsigned long long); MODE 4: the sum is
+// added to out (float, detector-column layout), one xy block's share of it;
+// MODE 5: MODE 3 within one xy block.  MODES 4 and 5 take the column's stretch
+// inside the xy block blk = {x planes blk.x .. blk.y, y planes blk.z .. blk.w},
+// the others the whole volume's.
+// g is read [view][v][u]; out is written in
 // the detector-column layout [view][u][v] when COLS (a warp's 32 rows store
 // 128 contiguous bytes), else [view][v][u].  A CTA takes detector column u of
 // one view and rows vstart .. vstart + kColRows - 1: from the tile list
@@ -337,7 +343,7 @@ __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const 
                                                              const ZParam* __restrict__ zp,
                                                              const float* __restrict__ wq,
                                                              const uint2* __restrict__ tiles, unsigned view0,
-                                                             const float* __restrict__ volz,
+                                                             int4 blk, const float* __restrict__ volz,
                                                              const GT* __restrict__ g, OT* __restrict__ out)
 {
     // piece j: {t where it ends, offset of its (x, y) voxel column in volz (int bits)}
@@ -357,15 +363,19 @@ __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const 
     const int Zp = G.Z + 2;
     const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
     const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
-    const float x0 = plane_t(0, T.x, T.y, K.x), x1 = plane_t(G.X, T.x, T.y, K.x);
-    const float y0 = plane_t(0, T.z, T.w, K.y), y1 = plane_t(G.Y, T.z, T.w, K.y);
+    constexpr bool COUNTING = MODE == 3 || MODE == 5;
+    const int4 b = MODE >= 4 ? blk : make_int4(0, G.X, 0, G.Y);
+    const float x0 = plane_t(b.x, T.x, T.y, K.x), x1 = plane_t(b.y, T.x, T.y, K.x);
+    const float y0 = plane_t(b.z, T.z, T.w, K.y), y1 = plane_t(b.w, T.z, T.w, K.y);
     const float t_in = fmaxf(fminf(x0, x1), fminf(y0, y1));
     const float t_out = fminf(fmaxf(x0, x1), fmaxf(y0, y1));
-    int n = 0;  // pieces; 0 when the column's rays miss the volume's xy footprint
+    int n = 0;  // pieces; 0 when the column's rays miss the block's xy footprint
     if (t_in < t_out) {
         const double ivx = 1.0 / (double)T.x, ivy = 1.0 / (double)T.z;
-        const int ix = locate<true>(t_in, T.x, T.y, K.x, G.X, ivx), ex = locate<false>(t_out, T.x, T.y, K.x, G.X, ivx);
-        const int iy = locate<true>(t_in, T.z, T.w, K.y, G.Y, ivy), ey = locate<false>(t_out, T.z, T.w, K.y, G.Y, ivy);
+        const int ix = locate_in<true>(t_in, T.x, T.y, K.x, b.x, b.y, ivx);
+        const int ex = locate_in<false>(t_out, T.x, T.y, K.x, b.x, b.y, ivx);
+        const int iy = locate_in<true>(t_in, T.z, T.w, K.y, b.z, b.w, ivy);
+        const int ey = locate_in<false>(t_out, T.z, T.w, K.y, b.z, b.w, ivy);
         const int nx = abs(ex - ix), ny = abs(ey - iy);
         n = nx + ny + 1;
         const int dx = T.x > 0.0f ? 1 : -1, dy = T.z > 0.0f ? 1 : -1;
@@ -406,29 +416,34 @@ __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const 
     const bool valid = v < vend;
     float2 sum = make_float2(0.0f, 0.0f);
     if (n > 0) {
-        if (MIRROR) sum = column_row_sum_mirror<KAHAN, MODE == 3>(G, zp, volz, spc, n, t_in, t_out, v, valid);
-        else sum.x = column_row_sum<KAHAN, MODE == 3>(G, zp, volz, spc, n, t_in, t_out, v, valid);
+        if (MIRROR) sum = column_row_sum_mirror<KAHAN, COUNTING>(G, zp, volz, spc, n, t_in, t_out, v, valid);
+        else sum.x = column_row_sum<KAHAN, COUNTING>(G, zp, volz, spc, n, t_in, t_out, v, valid);
     }
-    if (MODE == 3) {
+    if (COUNTING) {
         unsigned long long c = valid ? (unsigned long long)sum.x + (unsigned long long)sum.y : 0ull;
         for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
         if (lane == 0 && c) atomicAdd(reinterpret_cast<unsigned long long*>(out), c);
         return;
     }
     if (!valid) return;
-    if constexpr (MODE != 3) {
+    if constexpr (!COUNTING) {
         const size_t base = (size_t)(view - view0) * G.Nu * G.Nv;
         auto emit = [&](int row, float acc) {
             const size_t pix_rm = (size_t)row * G.Nu + u, pix_col = (size_t)u * G.Nv + row;
-            const float w = __ldg(wq + pix_col);
-            const float hf = w * acc;
-            OT* const o = out + base + (COLS ? pix_col : pix_rm);
-            if (MODE == 0) {
-                store_val<OT>(o, hf);
+            if constexpr (MODE == 4) {
+                static_assert(COLS, "block sums are kept in the detector-column layout");
+                out[base + pix_col] += acc;
             } else {
-                const float gv = load_val<GT>(g + base + pix_rm);
-                const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-                store_val<OT>(o, MODE == 1 ? ratio * w : ratio);
+                const float w = __ldg(wq + pix_col);
+                const float hf = w * acc;
+                OT* const o = out + base + (COLS ? pix_col : pix_rm);
+                if (MODE == 0) {
+                    store_val<OT>(o, hf);
+                } else {
+                    const float gv = load_val<GT>(g + base + pix_rm);
+                    const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
+                    store_val<OT>(o, MODE == 1 ? ratio * w : ratio);
+                }
             }
         };
         emit(v, sum.x);
@@ -456,6 +471,78 @@ __global__ void __launch_bounds__(256) to_zfast_kernel(const float* __restrict__
     }
 }
 
+// Bit b of mask[view][u]: detector column u's rays cross xy block b (blocks of
+// `side` voxels, nbx along x), by the column kernel's own test.
+__global__ void __launch_bounds__(128) column_block_mask_kernel(ExactGeom G, const float4* __restrict__ txy,
+                                                                const int2* __restrict__ kxy, unsigned nview, int side,
+                                                                int nbx, int nby,
+                                                                unsigned long long* __restrict__ mask)
+{
+    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (q >= (size_t)nview * G.Nu) return;
+    const float4 T = txy[q];
+    const int2 K = kxy[q];
+    unsigned long long m = 0ull;
+    for (int by = 0; by < nby; ++by)
+        for (int bx = 0; bx < nbx; ++bx) {
+            const float x0 = plane_t(bx * side, T.x, T.y, K.x), x1 = plane_t(min((bx + 1) * side, G.X), T.x, T.y, K.x);
+            const float y0 = plane_t(by * side, T.z, T.w, K.y), y1 = plane_t(min((by + 1) * side, G.Y), T.z, T.w, K.y);
+            if (fmaxf(fminf(x0, x1), fminf(y0, y1)) < fminf(fmaxf(x0, x1), fmaxf(y0, y1)))
+                m |= 1ull << (by * nbx + bx);
+        }
+    mask[q] = m;
+}
+
+// The blocks' summed ray sums acc ([view][u][v], from view0) into the forward
+// projector's output as fp_column_kernel's MODE writes it (0, 1 or 2), over
+// 32 (u) x 32 (v) tiles: g is read along u and acc, w along v; a row-major out
+// is written along u through the same tile.  acc may be out itself (float,
+// detector-column layout): each thread reads its pixel before writing it.
+template <int MODE, bool COLS, class GT, class OT>
+__global__ void __launch_bounds__(256) column_finish_kernel(ExactGeom G, const float* acc,
+                                                            const float* __restrict__ wq,
+                                                            const GT* __restrict__ g, OT* out)
+{
+    __shared__ float tile[32][33];
+    const int u0 = blockIdx.x * 32, v0 = blockIdx.y * 32;
+    const size_t base = (size_t)blockIdx.z * G.Nu * G.Nv;
+    if (MODE != 0) {
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int u = u0 + threadIdx.x, v = v0 + r;
+            if (u < G.Nu && v < G.Nv) tile[r][threadIdx.x] = load_val<GT>(g + base + (size_t)v * G.Nu + u);
+        }
+        __syncthreads();
+    }
+    float val[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int u = u0 + threadIdx.y + 8 * q, v = v0 + threadIdx.x;
+        val[q] = 0.0f;
+        if (u < G.Nu && v < G.Nv) {
+            const size_t pc = (size_t)u * G.Nv + v;
+            const float w = __ldg(wq + pc);
+            const float hf = w * acc[base + pc];
+            if (MODE == 0) {
+                val[q] = hf;
+            } else {
+                const float ratio = (hf != 0.0f) ? __fdiv_rn(tile[threadIdx.x][threadIdx.y + 8 * q], hf) : 0.0f;
+                val[q] = MODE == 1 ? ratio * w : ratio;
+            }
+            if (COLS) store_val<OT>(out + base + pc, val[q]);
+        }
+    }
+    if (!COLS) {
+        __syncthreads();  // the g tile is read
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tile[threadIdx.x][threadIdx.y + 8 * q] = val[q];
+        __syncthreads();
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int u = u0 + threadIdx.x, v = v0 + r;
+            if (u < G.Nu && v < G.Nv) store_val<OT>(out + base + (size_t)v * G.Nu + u, tile[r][threadIdx.x]);
+        }
+    }
+}
+
 }  // namespace exact
 
 // ---- host side -----------------------------------------------------------------------------
@@ -477,30 +564,107 @@ bool exact_fp_column_suits(const Plan& P)
            (size_t)(E.X + E.Y + 2) * sizeof(float2) <= 200 * 1024;
 }
 
+// Side of the xy blocks the column projector walks one at a time (0: the
+// whole volume in one pass).  AUTO: blocks when the z-fastest copy is larger
+// than 96 MiB, so that the CTAs in flight, which all take one block, read at
+// most 40 MiB of it and the 126 MB L2 holds their reads across views; at most
+// 64 blocks.  The option's n > 0 asks for n x n columns.
+static int column_block_side(const Plan& P)
+{
+    const ExactGeom& E = P.eg;
+    if (P.opt.fp_block < 0) return 0;
+    const double col_bytes = 4.0 * (E.Z + 2.0);
+    int side = P.opt.fp_block;
+    if (side == 0) {
+        if ((double)E.X * E.Y * col_bytes <= 96.0 * (1 << 20)) return 0;
+        side = std::max(8, (int)std::sqrt(40.0 * (1 << 20) / col_bytes) / 8 * 8);
+        side = std::max(side, (std::max(E.X, E.Y) + 7) / 8);
+    }
+    return (side >= E.X && side >= E.Y) ? 0 : side;
+}
+
+// The rows of view n's tiles: blocks of kColRows rows (from the first) inside
+// its rectangle of rays; mirror plans take the lower rows of the rectangle and
+// of its mirror image.
+static void column_rows(const Plan& P, const int4& r, int* v0, int* v1)
+{
+    const int Nv = P.eg.Nv;
+    *v0 = P.z_mirror ? std::min(r.z, Nv - 1 - r.w) : r.z;
+    *v1 = P.z_mirror ? std::min(std::max(r.w, Nv - 1 - r.z), Nv / 2 - 1) : r.w;
+}
+
+static recon_status_t upload_tiles(Plan& P, RayTiles& T, const std::vector<uint2>& tiles)
+{
+    if (tiles.empty()) return RECON_OK;
+    RB_CHECK(P.alloc(&T.d, tiles.size(), "column tiles"));
+    RB_CUDA(cudaMemcpy(T.d, tiles.data(), tiles.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    return RECON_OK;
+}
+
 // Tiles {view, u | vstart << 16} of the column kernel: per view, the columns and
-// blocks of kColRows rows (from the first) inside the rectangle of rays that
-// cross the volume.  rect is per plan view {u_min, u_max, v_min, v_max}.
+// row blocks inside the rectangle of rays that cross the volume (rect, per
+// plan view {u_min, u_max, v_min, v_max}); with xy blocks, one list per block
+// of the columns whose rays cross it.
 recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect)
 {
     const unsigned nv = P.nviews;
-    P.col_tiles.prefix.assign(nv + 1, 0);
-    std::vector<uint2> tiles;
-    const int Nv = P.eg.Nv;
+    const ExactGeom& E = P.eg;
+    P.col_block = column_block_side(P);
+    P.col_btiles.clear();
+    if (P.col_block == 0) {
+        P.col_tiles.prefix.assign(nv + 1, 0);
+        std::vector<uint2> tiles;
+        for (unsigned n = 0; n < nv; ++n) {
+            P.col_tiles.prefix[n] = (unsigned)tiles.size();
+            const int4 r = rect[n];
+            if (r.y < r.x) continue;
+            int v0, v1;
+            column_rows(P, r, &v0, &v1);
+            for (int u = r.x; u <= r.y; ++u)
+                for (int vs = v0; vs <= v1; vs += exact::kColRows)
+                    tiles.push_back(make_uint2(n, (unsigned)u | ((unsigned)vs << 16)));
+        }
+        P.col_tiles.prefix[nv] = (unsigned)tiles.size();
+        return upload_tiles(P, P.col_tiles, tiles);
+    }
+    const int side = P.col_block;
+    P.col_nbx = (E.X + side - 1) / side;
+    P.col_nby = (E.Y + side - 1) / side;
+    const int nb = P.col_nbx * P.col_nby;
+    if (nb > 64) return fail(RECON_ERR_INVALID_ARGUMENT, "fp_block: more than 64 xy blocks");
+    std::vector<unsigned long long> mask((size_t)nv * E.Nu, 0ull);
+    if (nv) {
+        unsigned long long* d_mask = nullptr;
+        RB_CUDA(cudaMalloc(&d_mask, mask.size() * sizeof(unsigned long long)));
+        const size_t nq = mask.size();
+        exact::column_block_mask_kernel<<<(unsigned)((nq + 127) / 128), 128>>>(E, P.d_txy, P.d_kxy, nv, side,
+                                                                             P.col_nbx, P.col_nby, d_mask);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpy(mask.data(), d_mask, nq * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        cudaFree(d_mask);
+        if (e != cudaSuccess) return cuda_fail(e, "column block masks");
+    }
+    P.col_btiles.resize(nb);
+    std::vector<std::vector<uint2>> tiles(nb);
+    for (int b = 0; b < nb; ++b) P.col_btiles[b].prefix.assign(nv + 1, 0);
     for (unsigned n = 0; n < nv; ++n) {
-        P.col_tiles.prefix[n] = (unsigned)tiles.size();
+        for (int b = 0; b < nb; ++b) P.col_btiles[b].prefix[n] = (unsigned)tiles[b].size();
         const int4 r = rect[n];
         if (r.y < r.x) continue;
-        // mirror plans: the lower rows of the rectangle and of its mirror image
-        const int v0 = P.z_mirror ? std::min(r.z, Nv - 1 - r.w) : r.z;
-        const int v1 = P.z_mirror ? std::min(std::max(r.w, Nv - 1 - r.z), Nv / 2 - 1) : r.w;
+        int v0, v1;
+        column_rows(P, r, &v0, &v1);
         for (int u = r.x; u <= r.y; ++u)
-            for (int vs = v0; vs <= v1; vs += exact::kColRows)
-                tiles.push_back(make_uint2(n, (unsigned)u | ((unsigned)vs << 16)));
+            for (unsigned long long m = mask[(size_t)n * E.Nu + u]; m; m &= m - 1) {
+                const int b = __builtin_ctzll(m);
+                for (int vs = v0; vs <= v1; vs += exact::kColRows)
+                    tiles[b].push_back(make_uint2(n, (unsigned)u | ((unsigned)vs << 16)));
+            }
     }
-    P.col_tiles.prefix[nv] = (unsigned)tiles.size();
-    if (tiles.empty()) return RECON_OK;
-    RB_CHECK(P.alloc(&P.col_tiles.d, tiles.size(), "column tiles"));
-    RB_CUDA(cudaMemcpy(P.col_tiles.d, tiles.data(), tiles.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    for (int b = 0; b < nb; ++b) {
+        P.col_btiles[b].prefix[nv] = (unsigned)tiles[b].size();
+        RB_CHECK(upload_tiles(P, P.col_btiles[b], tiles[b]));
+    }
     return RECON_OK;
 }
 
@@ -519,14 +683,83 @@ recon_status_t exact_to_zfast(const Plan& P, const float* vol, cudaStream_t s)
 // outside the tiles are zeroed; the MLEM ratio buffers are zero there from
 // allocation on.
 template <int MODE, bool COLS, class GT, class OT>
+static auto column_kernel(const Plan& P)
+{
+    const bool kahan = P.opt.sum == RECON_SUM_KAHAN;
+    auto kernel = P.z_mirror ? (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, true>
+                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, true>)
+                             : (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, false>
+                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, false>);
+    return kernel;
+}
+
+// Views [first, first + count) of plan views over the xy blocks: each block's
+// tiles add their stretch of the ray sums into acc (in launch order, so the sums
+// are deterministic), then column_finish_kernel forms the output; MODE 3 adds
+// each block's pair count.  acc is the output itself where that is float in
+// detector columns, else the plan's block-sum buffer.
+template <int MODE, bool COLS, class GT, class OT>
+static recon_status_t launch_column_blocks(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g,
+                                          OT* out, cudaStream_t s)
+{
+    const ExactGeom& E = P.eg;
+    const size_t smem = (size_t)(E.X + E.Y + 2) * sizeof(float2);
+    constexpr bool in_place = COLS && std::is_same<OT, float>::value;
+    float* acc = nullptr;
+    if (MODE != 3) {
+        if (in_place) {
+            acc = reinterpret_cast<float*>(out);
+        } else {
+            if (!P.d_col_acc) RB_CHECK(P.alloc(&P.d_col_acc, (size_t)P.nviews * P.npix, "column block sums"));
+            acc = P.d_col_acc;
+        }
+        RB_CUDA(cudaMemsetAsync(acc, 0, (size_t)count * P.npix * sizeof(float), s));
+        RB_CHECK(exact_to_zfast(P, vol, s));
+    }
+    constexpr int BMODE = MODE == 3 ? 5 : 4;
+    using BOT = typename std::conditional<MODE == 3, OT, float>::type;
+    auto kernel = column_kernel<BMODE, MODE == 3 ? COLS : true, float, BOT>(P);
+    if (smem > 48 * 1024) RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BOT* bout;
+    if constexpr (MODE == 3) bout = out;
+    else bout = acc;
+    const int side = P.col_block;
+    for (int by = 0; by < P.col_nby; ++by)
+        for (int bx = 0; bx < P.col_nbx; ++bx) {
+            const RayTiles& T = P.col_btiles[by * P.col_nbx + bx];
+            const unsigned t0 = T.prefix[first], nt = T.prefix[first + count] - t0;
+            if (nt == 0) continue;
+            const int4 blk = make_int4(bx * side, std::min((bx + 1) * side, E.X), by * side,
+                                       std::min((by + 1) * side, E.Y));
+            kernel<<<nt, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, T.d + t0, first, blk,
+                                                     P.d_vol_z, nullptr, bout);
+            RB_CUDA(cudaGetLastError());
+        }
+    if constexpr (MODE != 3) {
+        const dim3 grid((E.Nu + 31) / 32, (E.Nv + 31) / 32, count);
+        exact::column_finish_kernel<MODE, COLS, GT, OT><<<grid, dim3(32, 8), 0, s>>>(E, acc, P.d_wq, g, out);
+        RB_CUDA(cudaGetLastError());
+    }
+    return RECON_OK;
+}
+
+// Views [first, first + count) of table slots through the column kernel: the
+// tile list for plan views, the full grid otherwise (the scratch slot).  The
+// volume is copied to the z-fastest layout first.  For MODE 0 the pixels
+// outside the tiles are zeroed; the MLEM ratio buffers are zero there from
+// allocation on.  Plans with xy blocks take plan views block by block.
+template <int MODE, bool COLS, class GT, class OT>
 static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g, OT* out,
                                     cudaStream_t s)
 {
     if (count == 0) return RECON_OK;
     const ExactGeom& E = P.eg;
+    const bool plan_views = first + count <= P.nviews;
+    if (plan_views && P.col_block > 0 && P.col_btiles.size() == (size_t)P.col_nbx * P.col_nby)
+        return launch_column_blocks<MODE, COLS, GT, OT>(P, vol, first, count, g, out, s);
     dim3 grid;
     const uint2* tiles = nullptr;
-    if (first + count <= P.nviews && P.col_tiles.prefix.size() == P.nviews + 1) {
+    if (plan_views && P.col_tiles.prefix.size() == P.nviews + 1) {
         const unsigned t0 = P.col_tiles.prefix[first], nt = P.col_tiles.prefix[first + count] - t0;
         if (MODE == 0) RB_CUDA(cudaMemsetAsync(out, 0, (size_t)count * P.npix * sizeof(OT), s));
         if (nt == 0) return RECON_OK;
@@ -538,13 +771,10 @@ static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, u
     }
     if (MODE != 3) RB_CHECK(exact_to_zfast(P, vol, s));
     const size_t smem = (size_t)(E.X + E.Y + 2) * sizeof(float2);
-    const bool kahan = P.opt.sum == RECON_SUM_KAHAN;
-    auto kernel = P.z_mirror ? (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, true>
-                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, true>)
-                             : (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, false>
-                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, false>);
+    auto kernel = column_kernel<MODE, COLS, GT, OT>(P);
     if (smem > 48 * 1024) RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kernel<<<grid, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, tiles, first, P.d_vol_z, g, out);
+    kernel<<<grid, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, tiles, first,
+                                               make_int4(0, E.X, 0, E.Y), P.d_vol_z, g, out);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }

@@ -129,6 +129,13 @@ struct Plan {
     // back-projection z-slab; rays outside them contribute nothing
     RayTiles fp_tiles;
     RayTiles col_tiles;           // column forward projector: {view, u | vstart << 16} per CTA
+    // column forward projector over xy blocks (volumes larger than L2): block
+    // side in voxels (0: one pass over the whole volume), the blocks' tiles,
+    // and block sums [nviews][u][v] where the output cannot hold them
+    int col_block = 0;
+    int col_nbx = 1, col_nby = 1;
+    std::vector<RayTiles> col_btiles;
+    float* d_col_acc = nullptr;
     int4* d_view_rect = nullptr;  // [view] {u_min, u_max, v_min, v_max} of the rays crossing the volume
     std::vector<RayTiles> bp_tiles;
     TexCache tex;  // voxel-driven back projection
