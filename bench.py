@@ -51,6 +51,10 @@ def parse_args():
                     help="run only the batched-vs-plain leg and print it as the JSON line")
     ap.add_argument("--no-voxel", action="store_true", help="skip the voxel-driven back projector leg")
     ap.add_argument("--no-compat", action="store_true", help="skip the COMPAT (reference arithmetic) leg")
+    ap.add_argument("--large36", choices=["both", "whole", "blocks"],
+                    help="only the 512^3 / 1024x768 / 36-view forward and back step, with the column forward "
+                         "projector walking the volume whole (fp_block -1), in xy blocks (AUTO) or both; "
+                         "one JSON line per design")
     ap.add_argument("--batched-problems", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=20)
     return ap.parse_args()
@@ -333,6 +337,56 @@ def compat_leg(cfg, g, device_index: int, budget_s: float = 10.0):
             "arithmetic": "COMPAT (the reference's FP32 traversal; bit-exact per ray)"}
 
 
+def large36_leg(which: str, device_index: int):
+    """512^3 volume of 0.125 mm, 1024 x 768 detector of 0.25 mm, 36 consecutive views
+    at 0.5 deg, a seeded random volume in [0, 0.05): one MLEM forward step and one
+    back projection with the update, best of 3 by CUDA events after 3 warm-up
+    iterations, for the column forward projector over the whole volume and / or
+    in xy blocks.  With both, the pair counts and the two images after the 4
+    iterations are compared."""
+    import torch
+
+    from recon_b200 import PROJECTOR_FORWARD, Options, Plan
+    from recon_b200.configs import LARGE, scaled
+
+    cfg = scaled(LARGE, NumProj=36, DeltaAng=0.5)
+    gen = torch.Generator("cuda").manual_seed(1)
+    vol = torch.rand((512, 512, 512), device="cuda", generator=gen) * 0.05
+    sides = {"whole": [-1], "blocks": [0], "both": [-1, 0]}[which]
+    images = []
+    for side in sides:
+        P = Plan(cfg, Options(fp_block=side, device=device_index))
+        g = P.fp_views(vol)
+        P.mlem_prepare()
+        f = P.new_volume(1.0)
+        for _ in range(3):
+            P.mlem_forward(g, f)
+            P.mlem_backward_update(f)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(3):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
+            P.mlem_forward(g, f)
+            e[1].record()
+            P.mlem_backward_update(f)
+            e[2].record()
+            torch.cuda.synchronize()
+            ts.append((e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])))
+        line = {"workload": "large_512cube_36x1024x768", "fp_block": side, "forward_projector": P.forward_projector,
+                "forward_ms": min(t[0] for t in ts), "backward_ms": min(t[1] for t in ts)}
+        if which == "both":
+            line["pairs_forward"] = P.count_projector_pairs(PROJECTOR_FORWARD)
+            line["isects"] = P.count_intersections()
+            images.append(f.double())
+        print(json.dumps(line), flush=True)
+        del P, g, f
+        torch.cuda.empty_cache()
+    if len(images) == 2:
+        a, b = images
+        print(json.dumps({"image_rel_l2_blocks_vs_whole_after_4_iterations": ((a - b).norm() / a.norm()).item()}))
+
+
 def ref_view_seconds(R, O, geo, cfg, view, steps, f, gview, ht):
     """Seconds for one view of one MLEM iteration with the reference's
     step-synchronous kernels built for the host, from a timed prefix of
@@ -500,6 +554,10 @@ def main():
     from recon_b200.sharding import sharded_mlem_iteration, view_range
 
     world, rank, local = dist_env()
+    if args.large36:
+        torch.cuda.set_device(local)
+        large36_leg(args.large36, local)
+        return
     if args.batched_only:
         torch.cuda.set_device(local)
         opts = Options(sum=SUM_KAHAN if args.sum == "kahan" else SUM_PLAIN, device=local)
