@@ -256,8 +256,33 @@ def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int
     t_batch = e0.elapsed_time(e1) * 1e-3
     t_plain = e1.elapsed_time(e2) * 1e-3
     same = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(fb, fp))
-    isects = sum(P.count_intersections() for P in plans)
+    isects_each = [P.count_intersections() for P in plans]
+    isects = sum(isects_each)
     n_gather = sum(1 for P in plans if P.siddon_bp == SIDDON_BP_GATHER)
+    # each problem's forward step and back projection timed alone (after the
+    # comparison above): what the batch can at best add up to
+    alone = []
+    for P, g, f in zip(plans, gs, fp):
+        P.mlem_forward(g, f)
+        P.mlem_backward_update(f)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        P.mlem_forward(g, f)
+        e[1].record()
+        P.mlem_backward_update(f)
+        e[2].record()
+        torch.cuda.synchronize()
+        alone.append((e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])))
+    bins = []
+    for lo, hi in ((0, 30), (30, 60), (60, 120), (120, None)):
+        sel = [k for k, c in enumerate(cfgs)
+               if lo <= isects_each[k] / (c["Xdim"] * c["Ydim"] * c["NumProj"]) < (hi or float("inf"))]
+        if sel:
+            n_is = sum(isects_each[k] for k in sel)
+            bins.append({"isects_per_column_view": [lo, hi], "problems": len(sel),
+                         "fp_isects_per_s": n_is / (1e-3 * sum(alone[k][0] for k in sel)),
+                         "bp_isects_per_s": n_is / (1e-3 * sum(alone[k][1] for k in sel))})
+    alone_s = 1e-3 * sum(a + b for a, b in alone)
     if world > 1:
         import torch.distributed as dist
 
@@ -275,6 +300,8 @@ def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int
         "speedup": t_plain / t_batch, "batched_isects_per_s": 2.0 * isects * iters / t_batch,
         "plain_isects_per_s": 2.0 * isects * iters / t_plain, "bitwise_equal": bool(same),
         "back_projectors": {"gather": n_gather, "ray": len(plans) - n_gather, "choice": "measured per geometry"},
+        "alone": {"serial_iter_s": len(plans) / alone_s, "isects_per_s": 2.0 * isects / alone_s, "by_work": bins,
+                  "note": "each problem's forward step and back projection timed alone on this rank"},
         "sharding": f"problems by rank over {world} GPUs" if world > 1 else "single GPU",
         "config": {"workload": f"batched_{n_prob}_seed4", "voxels_min_max": [min(vox), max(vox)],
                    "views_min_max": [min(int(c["NumProj"]) for c in cfgs), max(int(c["NumProj"]) for c in cfgs)],
