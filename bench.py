@@ -450,10 +450,24 @@ def cpu_baseline(cfg, g_host, steps: int = 24):
     view = n // 10
     t_view, dt, loopN, s = ref_view_seconds(R, O, geo, cfg, view, steps, f,
                                             np.ascontiguousarray(g_host[view].ravel()), ht)
-    return {"value": 1.0 / (t_view * n), "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"view {view} of one MLEM iteration (FP + ratio + BP with the reference's step-synchronous "
-                      f"kernels built for the host): the first {s} of its {loopN} step launches took {dt:.1f} s, "
-                      f"scaled by (loopN+1)/(steps+1) to {t_view:.0f} s/view and by {n} views"}
+    out = {"value": 1.0 / (t_view * n), "unit": UNIT, "cores": 1, "kind": "reference",
+           "sample": f"view {view} of one MLEM iteration (FP + ratio + BP with the reference's step-synchronous "
+                     f"kernels built for the host): the first {s} of its {loopN} step launches took {dt:.1f} s, "
+                     f"scaled by (loopN+1)/(steps+1) to {t_view:.0f} s/view and by {n} views"}
+    # the per-ray FP64 Siddon oracle (one thread per view group), for scale
+    vol = np.ones(geo.nvox)
+    fp64 = {}
+    cores = os.cpu_count() or 1
+    for label, threads, nv in (("1_core", 1, 4), ("all_cores", cores, max(4, 2 * cores))):
+        t0 = time.perf_counter()
+        sino = O.x_fp_all(geo, nv, 360.0 / nv, vol, threads)
+        O.x_bp_all(geo, nv, 360.0 / nv, sino, threads)
+        fp64[label] = nv / ((time.perf_counter() - t0) * n)
+    out["fp64_oracle"] = {"iter_s_1_core": fp64["1_core"], "iter_s_all_cores": fp64["all_cores"],
+                          "cores": cores, "unit": UNIT,
+                          "sample": f"FP + BP with the per-ray FP64 Siddon oracle of 4 evenly spaced views on one "
+                                    f"thread and of max(4, 2 x cores) on all, extrapolated to {n} views"}
+    return out
 
 
 def reference_gpu_leg(O, geo, cfg, vol, gviews: dict) -> dict | None:

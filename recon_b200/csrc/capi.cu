@@ -198,6 +198,13 @@ recon_status_t ensure_mlem_buffers(Plan& P)
             P.d_ratio_rm = q;
         }
     }
+    // block sums of the column forward projector where the ratio cannot hold
+    // them (allocated here, before any graph capture of an iteration)
+    if (P.opt.arith == RECON_ARITH_EXACT && P.fp_column && P.col_block > 0 && !P.d_col_acc) {
+        const bool in_place =
+            P.opt.sino == RECON_SINO_F32 && (mlem_ratio_in_columns(P) || voxel_ratio_in_columns(P));
+        if (!in_place) RB_CHECK(P.alloc(&P.d_col_acc, (size_t)P.nviews * P.npix, "column block sums"));
+    }
     return RECON_OK;
 }
 

@@ -42,8 +42,8 @@ def test_exports_every_declared_function():
 def test_default_options():
     o = L.Options()
     assert L.lib().recon_default_options(C.byref(o)) == 0
-    assert (o.arith, o.sum, o.sino, o.bp, o.voxel_mode, o.device, o.siddon_bp) == (
-        L.ARITH_EXACT, L.SUM_KAHAN, L.SINO_F32, L.BP_SIDDON, L.VOXEL_GEOMETRIC, 0, L.SIDDON_BP_AUTO)
+    assert (o.arith, o.sum, o.sino, o.bp, o.voxel_mode, o.device, o.siddon_bp, o.fp_block) == (
+        L.ARITH_EXACT, L.SUM_KAHAN, L.SINO_F32, L.BP_SIDDON, L.VOXEL_GEOMETRIC, 0, L.SIDDON_BP_AUTO, 0)
 
 
 def _cfg_text(extra=""):
@@ -142,6 +142,11 @@ def test_plan_rejects_bad_geometry():
     assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1
     o.arith, o.siddon_bp = 0, 4  # 0..3 are AUTO, GATHER, RAY, TUNED
     assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1
+    o.siddon_bp = 0
+    for bad_block in (-2, 3):  # -1 = never, 0 = AUTO; 3 gives 11 x 11 > 64 blocks of the 32 x 32 columns
+        o.fp_block = bad_block
+        assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1, bad_block
+        assert "fp_block" in lib.recon_last_error().decode()
 
 
 @pytest.mark.skipif(have_gpu(), reason="checks the no-device path")

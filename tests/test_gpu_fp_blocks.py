@@ -94,3 +94,34 @@ def test_blocked_mlem_iteration(name, sino):
 def test_block_count_limit():
     with pytest.raises(ReconError):
         Plan(small_cfg(), Options(fp_block=3))  # 11 x 11 blocks
+
+
+def test_blocked_osem_voxel_and_batch():
+    """The other callers of the forward projector with blocks: OSEM (view
+    subsets), the voxel-driven back projector's ratio (g / Hf) and a batch,
+    which must give the bits of its plain plans."""
+    from recon_b200 import BP_VOXEL, VOXEL_GEOMETRIC, Batch
+
+    cfg, side, _ = GEOMS["mirror"]
+    B, U = _plans(cfg, side)
+    vol = _volume(B, 73) + 0.2
+    g = U.fp_views(vol)
+    fb, fu = B.osem(g, 2, 3), U.osem(g, 2, 3)
+    err = rel_l2(fb.double().cpu().numpy(), fu.double().cpu().numpy())
+    assert err < 1e-6, err
+    VB = Plan(cfg, Options(fp_block=side, bp=BP_VOXEL, voxel_mode=VOXEL_GEOMETRIC))
+    VU = Plan(cfg, Options(fp_block=-1, bp=BP_VOXEL, voxel_mode=VOXEL_GEOMETRIC))
+    assert VB.forward_projector == FP_COLUMN_BLOCKS
+    vb, vu = VB.mlem(g, 2), VU.mlem(g, 2)
+    err = rel_l2(vb.double().cpu().numpy(), vu.double().cpu().numpy())
+    assert err < 1e-6, err
+    cfgs = [cfg, small_cfg(Xdim=30, Ydim=27, Zdim=24)]
+    opts = Options(fp_block=8)
+    plans = [Plan(c, opts) for c in cfgs]
+    assert all(P.forward_projector == FP_COLUMN_BLOCKS for P in plans)
+    gs = [P.fp_views(_volume(P, 74 + k) + 0.2) for k, P in enumerate(plans)]
+    batch = Batch(cfgs, opts).mlem(gs, 3)
+    for P, gk, fk in zip(plans, gs, batch):
+        ref = P.mlem(gk, 3)
+        torch.cuda.synchronize()
+        assert torch.equal(fk.view(torch.int32), ref.view(torch.int32))
