@@ -271,6 +271,20 @@ recon_status_t recon_mlem(recon_plan_t plan, const void* d_g, unsigned int iters
 recon_status_t recon_mlem_prepare(recon_plan_t plan, void* stream);
 recon_status_t recon_mlem_iteration(recon_plan_t plan, const void* d_g, float* d_f, void* stream);
 
+/* Copies views [first, first + count) of a measured sinogram [view][v][u]
+ * (element type as the plan's `sino` option) from host memory h_g to device
+ * memory d_g, both holding all NumProj views: for EXACT plans only detector
+ * rows v_min..v_max, the rows some ray crossing the volume reaches in some
+ * view, as one strided copy; the other rows of d_g are left as they are (no
+ * projector or MLEM call of the plan reads a value there: their rays miss the
+ * volume, so their ratio is 0 whatever g holds).  COMPAT plans copy whole
+ * views.  *bytes (may be NULL) receives the bytes copied.  Asynchronous on
+ * `stream`; pinned host memory lets the copy overlap compute.  No counterpart
+ * in the reference, which reads every view from disk every iteration
+ * (hf_siddon_recon.hpp:437-476). */
+recon_status_t recon_upload_sinogram(recon_plan_t plan, const void* h_g, void* d_g, unsigned first,
+                                     unsigned count, size_t* bytes, void* stream);
+
 /* The two halves of an iteration over a range of views, for callers that
  * split the views between devices (sum the partial Ht across devices, then
  * apply recon_mlem_update everywhere).  EXACT arithmetic, Siddon back

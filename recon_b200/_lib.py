@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
         "recon_mlem_prepare": (st, [P, P]),
         "recon_osem": (st, [P, P, u, u, P, C.c_int, P]),
         "recon_mlem_iteration": (st, [P, P, P, P]),
+        "recon_upload_sinogram": (st, [P, P, P, u, u, C.POINTER(C.c_size_t), P]),
         "recon_mlem_forward": (st, [P, P, P, u, u, P]),
         "recon_mlem_backward": (st, [P, u, u, P, P]),
         "recon_mlem_update": (st, [P, P, P, P]),
@@ -157,6 +158,7 @@ def exported_symbols() -> list[str]:
         "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_view_step_count", "recon_mlem_from_cfg",
         "recon_forward_projection_from_cfg", "recon_backward_projection_from_cfg", "recon_batch_create",
         "recon_batch_destroy", "recon_batch_mlem", "recon_compat_bp_view_noalloc", "recon_osem",
+        "recon_upload_sinogram",
     ]
 
 

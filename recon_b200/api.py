@@ -220,6 +220,26 @@ class Plan:
     def mlem_iteration(self, g, f) -> None:
         check(lib().recon_mlem_iteration(self._h, _ptr(g), _ptr(f), _stream()))
 
+    def upload_sinogram(self, g_host, g_dev, first: int = 0, count: int | None = None) -> int:
+        """recon_upload_sinogram: views [first, first + count) of the host sinogram
+        g_host into g_dev (both [NumProj][TAxPixels][AxPixels] in the plan's
+        sinogram type), only the rows the plan's rays can read; returns the
+        bytes copied.  Asynchronous on the current stream."""
+        count = self.nproj - first if count is None else count
+        if g_host.is_cuda or not g_dev.is_cuda:
+            raise ValueError("g_host must be in host memory and g_dev on the device")
+        if tuple(g_host.shape) != (self.nproj, self.nv, self.nu) or g_dev.shape != g_host.shape:
+            raise ValueError("g_host and g_dev must both be [NumProj][TAxPixels][AxPixels]")
+        es = 2 if self.options.sino == L.SINO_BF16 else 4
+        if g_host.dtype != g_dev.dtype or g_host.element_size() != es:
+            raise ValueError("g_host and g_dev must both have the plan's sinogram type")
+        if not g_host.is_contiguous():
+            raise ValueError("g_host must be contiguous")
+        n = C.c_size_t()
+        check(lib().recon_upload_sinogram(self._h, g_host.data_ptr(), _ptr(g_dev), first, count, C.byref(n),
+                                          _stream()))
+        return int(n.value)
+
     def mlem_forward(self, g, f, first: int = 0, count: int | None = None) -> None:
         count = self.nproj - first if count is None else count
         check(lib().recon_mlem_forward(self._h, _ptr(g), _ptr(f), first, count, _stream()))

@@ -185,8 +185,7 @@ recon_status_t ensure_mlem_buffers(Plan& P)
     if (!P.d_sens) RB_CHECK(P.alloc(&P.d_sens, P.nvox, "sensitivity"));
     if (!P.d_ratio) {
         const size_t es = (P.opt.sino == RECON_SINO_BF16) ? 2 : 4;
-        const bool per_view = (P.opt.arith == RECON_ARITH_COMPAT) && (P.opt.bp == RECON_BP_SIDDON);
-        const size_t n = per_view ? P.npix : (size_t)P.nviews * P.npix;
+        const size_t n = (size_t)P.nviews * P.npix;
         char* q = nullptr;
         RB_CHECK(P.alloc(&q, n * es, "ratio sinogram"));
         // zero outside the ray blocks the forward projector writes (EXACT culling)
@@ -319,7 +318,7 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(build_exact_culling(*P));
             if (tuned) RB_CHECK(exact_tune_bp(*P));
         } else {
-            RB_CHECK(P->alloc(&P->d_maxabs, nv1, "maxabs"));
+            RB_CHECK(P->alloc(&P->d_maxabs, nv1 + 1, "maxabs"));  // per view, scratch slot, all views
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));
             RB_CHECK(P->alloc(&P->d_ht, P->nvox, "Ht"));
             RB_CUDA(cudaMemset(P->d_fix, 0, P->nvox * sizeof(unsigned long long)));
@@ -486,6 +485,29 @@ recon_status_t recon_mlem_iteration(recon_plan_t P, const void* d_g, float* d_f,
     RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, s, 0, P->nviews));
     return exact_bp(*P, P->d_ratio, true, P->opt.sino == RECON_SINO_BF16, 0, P->nviews, false, false, nullptr,
                     P->d_sens, d_f, s);
+}
+
+recon_status_t recon_upload_sinogram(recon_plan_t P, const void* h_g, void* d_g, unsigned first, unsigned count,
+                                     size_t* bytes, void* stream)
+{
+    if (bytes) *bytes = 0;
+    if (!P || !h_g || !d_g) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    if ((size_t)first + count > P->nviews) return fail(RECON_ERR_INVALID_ARGUMENT, "view range beyond NumProj");
+    if (count == 0) return RECON_OK;
+    RB_CHECK(use_device(*P));
+    const size_t es = P->opt.sino == RECON_SINO_BF16 ? 2 : 4;
+    const size_t Nu = P->geom.det.NumAxPixels, Nv = P->geom.det.NumTAxPixels;
+    size_t row0 = 0, rows = Nv;
+    if (P->opt.arith == RECON_ARITH_EXACT && P->sino_rows_known) {
+        if (P->sino_v1 < P->sino_v0) return RECON_OK;  // no ray crosses the volume
+        row0 = (size_t)P->sino_v0;
+        rows = (size_t)(P->sino_v1 - P->sino_v0 + 1);
+    }
+    const size_t pitch = Nu * Nv * es, width = rows * Nu * es, off = ((size_t)first * Nv + row0) * Nu * es;
+    RB_CUDA(cudaMemcpy2DAsync(static_cast<char*>(d_g) + off, pitch, static_cast<const char*>(h_g) + off, pitch, width,
+                              count, cudaMemcpyHostToDevice, as_stream(stream)));
+    if (bytes) *bytes = width * count;
+    return RECON_OK;
 }
 
 static recon_status_t split_ok(recon_plan_t P, unsigned first, unsigned count)

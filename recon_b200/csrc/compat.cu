@@ -385,15 +385,19 @@ __device__ __forceinline__ double fix_scale(unsigned maxabs_bits, float max_len,
 // Back projection scatter: per in-range segment, len*img[n] added in 64-bit
 // fixed point (siddon_bp_calc_ray_path + the atomic kernel,
 // siddon_kernelsMLEM.cuh:307-365).
+// Views view0 + blockIdx.z, view z reading img + z * img_stride, all scaled by
+// maxabs[slot] (one view's bound, or the bound over all the views launched).
 __global__ void bp_scatter_kernel(CompatGeom G, const float* __restrict__ angles, const unsigned* __restrict__ loopN,
-                                  unsigned view, const float* __restrict__ img, const unsigned* __restrict__ maxabs,
-                                  float chord, int count_bits, unsigned long long* __restrict__ acc)
+                                  unsigned view0, const float* __restrict__ img, size_t img_stride,
+                                  const unsigned* __restrict__ maxabs, unsigned slot, float chord, int count_bits,
+                                  unsigned long long* __restrict__ acc)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int v = blockIdx.y * blockDim.y + threadIdx.y;
     if (u >= G.Nu || v >= G.Nv) return;
-    const size_t n = (size_t)u + (size_t)v * G.Nu;
-    const double scale = fix_scale(maxabs[view], chord, count_bits);
+    const unsigned view = view0 + blockIdx.z;
+    const size_t n = (size_t)blockIdx.z * img_stride + (size_t)u + (size_t)v * G.Nu;
+    const double scale = fix_scale(maxabs[slot], chord, count_bits);
     if (scale == 0.0) return;
     Ray r;
     setup(G, view_angle(angles, view), u, v, r);
@@ -436,6 +440,22 @@ __global__ void bp_finish_kernel(unsigned long long* __restrict__ acc, size_t n,
             acc[i] = 0ull;
         }
         out[i] = accumulate ? __fadd_rn(out[i], v) : v;
+    }
+}
+
+// out = max over views of maxabs[0 .. n) (non-negative floats as unsigned bits)
+__global__ void max_views_kernel(const unsigned* __restrict__ maxabs, unsigned n, unsigned* __restrict__ out)
+{
+    unsigned m = 0;
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) m = max(m, maxabs[i]);
+    m = __reduce_max_sync(0xffffffffu, m);
+    __shared__ unsigned w[32];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned r = 0;
+        for (unsigned k = 0; k < (blockDim.x + 31) / 32; ++k) r = max(r, w[k]);
+        *out = r;
     }
 }
 
@@ -514,8 +534,8 @@ static recon_status_t compat_bp_into(Plan& P, const float* img, unsigned view, f
         compat::maxabs_kernel<<<elem_blocks(P.npix), 256, 0, s>>>(img, P.npix, P.d_maxabs + view);
         RB_CUDA(cudaGetLastError());
     }
-    compat::bp_scatter_kernel<<<ray_grid(P, 1), ray_block(), 0, s>>>(P.cg, angles_dev(P), P.d_loopN, view, img,
-                                                                      P.d_maxabs, chord, cbits, P.d_fix);
+    compat::bp_scatter_kernel<<<ray_grid(P, 1), ray_block(), 0, s>>>(P.cg, angles_dev(P), P.d_loopN, view, img, 0,
+                                                                      P.d_maxabs, view, chord, cbits, P.d_fix);
     RB_CUDA(cudaGetLastError());
     compat::bp_finish_kernel<<<elem_blocks(P.nvox), 256, 0, s>>>(P.d_fix, P.nvox, P.d_maxabs, view, chord, cbits,
                                                                   out, accumulate ? 1 : 0);
@@ -533,27 +553,55 @@ recon_status_t compat_bp_view(Plan& P, const float* img, unsigned view, bool scr
     return compat_bp_into(P, img, view, out, accumulate, false, s);
 }
 
-recon_status_t compat_sensitivity(Plan& P, float* sens, cudaStream_t s)
+// Back projection of every plan view's image (img + n * img_stride) summed in
+// one 64-bit fixed-point accumulator, scaled by the bound over all views
+// (maxabs[nviews + 1], which the caller sets), and rounded to float once into
+// out.  The reference adds each view's back projection into a float image
+// (hf_siddon_recon.hpp:437-476); one rounding of the exact sum differs from
+// that by float rounding only.
+static recon_status_t compat_bp_all(Plan& P, const float* img, size_t img_stride, float* out, cudaStream_t s)
 {
-    RB_CHECK(launch_fill(P.d_view_img, 1.0f, P.npix, s));
-    RB_CUDA(cudaMemsetAsync(sens, 0, P.nvox * sizeof(float), s));
-    for (unsigned n = 0; n < P.nviews; ++n) RB_CHECK(compat_bp_into(P, P.d_view_img, n, sens, true, false, s));
+    const float chord = max_ray_length(P);
+    int cbits = count_bits(P);
+    while ((1u << (cbits - count_bits(P))) < P.nviews) ++cbits;  // contributions of every view
+    const unsigned all = P.nviews + 1;
+    compat::bp_scatter_kernel<<<ray_grid(P, P.nviews), ray_block(), 0, s>>>(P.cg, angles_dev(P), P.d_loopN, 0u, img,
+                                                                             img_stride, P.d_maxabs, all, chord, cbits,
+                                                                             P.d_fix);
+    RB_CUDA(cudaGetLastError());
+    compat::bp_finish_kernel<<<elem_blocks(P.nvox), 256, 0, s>>>(P.d_fix, P.nvox, P.d_maxabs, all, chord, cbits, out,
+                                                                  0);
+    RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
 
-// m_mlem_single_iteration (hf_siddon_recon.hpp:437-476): per view FP, ratio,
-// BP accumulated into Ht in view order; then f = f*Ht; f = divide1(f, sens).
+recon_status_t compat_sensitivity(Plan& P, float* sens, cudaStream_t s)
+{
+    if (P.nviews == 0) {
+        RB_CUDA(cudaMemsetAsync(sens, 0, P.nvox * sizeof(float), s));
+        return RECON_OK;
+    }
+    RB_CHECK(launch_fill(P.d_view_img, 1.0f, P.npix, s));
+    set_value_kernel<<<1, 1, 0, s>>>(reinterpret_cast<float*>(P.d_maxabs + P.nviews + 1), 1.0f);
+    RB_CUDA(cudaGetLastError());
+    return compat_bp_all(P, P.d_view_img, 0, sens, s);
+}
+
+// m_mlem_single_iteration (hf_siddon_recon.hpp:437-476): FP and ratio of every
+// view (the image is fixed within the iteration, so the views' order does not
+// matter), the back projections of all ratios summed exactly, then
+// f = f*Ht; f = divide1(f, sens).
 recon_status_t compat_mlem_iteration(Plan& P, const float* g, float* f, cudaStream_t s)
 {
-    RB_CUDA(cudaMemsetAsync(P.d_ht, 0, P.nvox * sizeof(float), s));
-    RB_CUDA(cudaMemsetAsync(P.d_maxabs, 0, (P.nviews + 1) * sizeof(unsigned), s));
+    if (P.nviews == 0) return RECON_OK;
+    RB_CUDA(cudaMemsetAsync(P.d_maxabs, 0, (P.nviews + 2) * sizeof(unsigned), s));
     float* ratio = static_cast<float*>(P.d_ratio);
-    for (unsigned n = 0; n < P.nviews; ++n) {
-        compat::fp_kernel<1><<<ray_grid(P, 1), ray_block(), 0, s>>>(P.cg, angles_dev(P), P.d_loopN, n, f,
-                                                                     g + (size_t)n * P.npix, ratio, P.d_maxabs);
-        RB_CUDA(cudaGetLastError());
-        RB_CHECK(compat_bp_into(P, ratio, n, P.d_ht, true, true, s));
-    }
+    compat::fp_kernel<1><<<ray_grid(P, P.nviews), ray_block(), 0, s>>>(P.cg, angles_dev(P), P.d_loopN, 0u, f, g, ratio,
+                                                                        P.d_maxabs);
+    RB_CUDA(cudaGetLastError());
+    compat::max_views_kernel<<<1, 256, 0, s>>>(P.d_maxabs, P.nviews, P.d_maxabs + P.nviews + 1);
+    RB_CUDA(cudaGetLastError());
+    RB_CHECK(compat_bp_all(P, ratio, P.npix, P.d_ht, s));
     return launch_update(f, P.d_ht, P.d_sens, P.nvox, true, s);
 }
 

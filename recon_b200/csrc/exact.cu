@@ -1018,6 +1018,14 @@ recon_status_t build_exact_culling(Plan& P)
 {
     std::vector<int4> rect;
     RB_CHECK(build_ray_tiles(P, 0, P.eg.Z, P.fp_tiles, &P.d_view_rect, &rect));
+    P.sino_v0 = INT_MAX;
+    P.sino_v1 = -1;
+    for (const int4& r : rect)
+        if (r.y >= r.x) {
+            P.sino_v0 = std::min(P.sino_v0, r.z);
+            P.sino_v1 = std::max(P.sino_v1, r.w);
+        }
+    P.sino_rows_known = true;
     if (P.fp_column && P.nviews) RB_CHECK(build_column_tiles(P, rect));
     P.bp_tiles.clear();
     if (P.bp_gather) return RECON_OK;  // the gather back projector needs no ray blocks

@@ -137,6 +137,8 @@ struct Plan {
     std::vector<RayTiles> col_btiles;
     float* d_col_acc = nullptr;
     int4* d_view_rect = nullptr;  // [view] {u_min, u_max, v_min, v_max} of the rays crossing the volume
+    int sino_v0 = 0, sino_v1 = -1;  // rows some ray crossing the volume reaches, over all views
+    bool sino_rows_known = false;   // EXACT culling ran: sino_v0..sino_v1 bound every row the plan reads
     std::vector<RayTiles> bp_tiles;
     TexCache tex;  // voxel-driven back projection
     // scratch view slot for arbitrary-angle single-view calls (index nviews)
