@@ -487,6 +487,45 @@ static int count_bits(const Plan& P)
     return b + 1;
 }
 
+// Scale bounds for the sum over all plan views (compat_bp_all).  A segment
+// lies on its ray between the volume's entry and exit, so it is no longer
+// than the volume's diagonal.  A contribution to a voxel comes from a ray
+// whose segment midpoint falls in it, i.e. a ray through the voxel's box (up
+// to the index rounding): with an untilted detector those are the pixels in
+// the box's shadow, at most W x H on the detector from the nearest depth the
+// volume reaches, widened by three pixels each way, with at most four segments
+// each.  A tilted detector falls back to one contribution per ray of the view.
+static float volume_diagonal(const Plan& P)
+{
+    const recon_geometry_t& g = P.geom;
+    const double x = g.vox.Xdim * (double)g.vox.XVoxSize, y = g.vox.Ydim * (double)g.vox.YVoxSize,
+                 z = g.vox.Zdim * (double)g.vox.ZVoxSize;
+    return (float)(std::sqrt(x * x + y * y + z * z) * 1.001 + 1e-3);
+}
+
+static int count_bits_all(const Plan& P)
+{
+    const recon_geometry_t& g = P.geom;
+    double per_view = std::ldexp(1.0, count_bits(P));
+    if (g.cal.xangle == 0.0f && g.cal.yangle == 0.0f && g.cal.zangle == 0.0f) {
+        const double vx = std::fabs((double)g.vox.XVoxSize), vy = std::fabs((double)g.vox.YVoxSize),
+                     vz = std::fabs((double)g.vox.ZVoxSize);
+        const double rmax = 0.5 * std::hypot(g.vox.Xdim * vx, g.vox.Ydim * vy);
+        const double dmin = std::fabs((double)g.cal.Rf) - rmax;
+        const double pu = std::fabs((double)g.det.AxPixDimMm * g.cal.M), pv = std::fabs((double)g.det.TAxPixDimMm * g.cal.M);
+        if (dmin > 0.0 && pu > 0.0 && pv > 0.0) {
+            const double mag = std::max(std::fabs((double)g.cal.R), std::fabs((double)g.cal.Ry)) / dmin;
+            const double diag = std::hypot(vx, vy), zmax = 0.5 * g.vox.Zdim * vz;
+            const double W = diag * mag, H = (vz + diag * zmax / dmin) * mag;
+            per_view = std::min(per_view, 4.0 * (std::ceil(W / pu) + 6.0) * (std::ceil(H / pv) + 6.0));
+        }
+    }
+    const double total = per_view * std::max(1u, P.nviews);
+    int b = 0;
+    while (std::ldexp(1.0, b) < total) ++b;
+    return b + 1;
+}
+
 __global__ void set_value_kernel(float* p, float v) { *p = v; }
 
 static float* angles_dev(Plan& P) { return P.d_angles; }
@@ -561,9 +600,8 @@ recon_status_t compat_bp_view(Plan& P, const float* img, unsigned view, bool scr
 // that by float rounding only.
 static recon_status_t compat_bp_all(Plan& P, const float* img, size_t img_stride, float* out, cudaStream_t s)
 {
-    const float chord = max_ray_length(P);
-    int cbits = count_bits(P);
-    while ((1u << (cbits - count_bits(P))) < P.nviews) ++cbits;  // contributions of every view
+    const float chord = volume_diagonal(P);
+    const int cbits = count_bits_all(P);
     const unsigned all = P.nviews + 1;
     compat::bp_scatter_kernel<<<ray_grid(P, P.nviews), ray_block(), 0, s>>>(P.cg, angles_dev(P), P.d_loopN, 0u, img,
                                                                              img_stride, P.d_maxabs, all, chord, cbits,
