@@ -185,7 +185,7 @@ recon_status_t ensure_mlem_buffers(Plan& P)
     if (!P.d_sens) RB_CHECK(P.alloc(&P.d_sens, P.nvox, "sensitivity"));
     if (!P.d_ratio) {
         const size_t es = (P.opt.sino == RECON_SINO_BF16) ? 2 : 4;
-        const size_t n = (size_t)P.nviews * P.npix;
+        const size_t n = (size_t)P.nviews * column_view_elems(P);
         char* q = nullptr;
         RB_CHECK(P.alloc(&q, n * es, "ratio sinogram"));
         // zero outside the ray blocks the forward projector writes (EXACT culling)
@@ -200,8 +200,8 @@ recon_status_t ensure_mlem_buffers(Plan& P)
     // block sums of the column forward projector where the ratio cannot hold
     // them (allocated here, before any graph capture of an iteration)
     if (P.opt.arith == RECON_ARITH_EXACT && P.fp_column && P.col_block > 0 && !P.d_col_acc) {
-        const bool in_place =
-            P.opt.sino == RECON_SINO_F32 && (mlem_ratio_in_columns(P) || voxel_ratio_in_columns(P));
+        const bool in_place = P.opt.sino == RECON_SINO_F32 && !P.col_pairs &&
+                              (mlem_ratio_in_columns(P) || voxel_ratio_in_columns(P));
         if (!in_place) RB_CHECK(P.alloc(&P.d_col_acc, (size_t)P.nviews * P.npix, "column block sums"));
     }
     return RECON_OK;
@@ -316,7 +316,10 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             RB_CHECK(exact_check_mirror(*P));
             if (tuned) P->bp_gather = false;  // the culling builds the ray design's slab tiles too
             RB_CHECK(build_exact_culling(*P));
+            const bool pairs = exact_pairs_suit(*P) && (P->bp_gather || tuned);
+            if (pairs) RB_CHECK(build_wq_pairs(*P));
             if (tuned) RB_CHECK(exact_tune_bp(*P));
+            P->col_pairs = pairs && P->bp_gather;
         } else {
             RB_CHECK(P->alloc(&P->d_maxabs, nv1 + 1, "maxabs"));  // per view, scratch slot, all views
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));
@@ -537,7 +540,7 @@ recon_status_t recon_mlem_backward(recon_plan_t P, unsigned first, unsigned coun
     cudaStream_t s = as_stream(stream);
     if (count == 0) return launch_fill(d_ht, 0.0f, P->nvox, s);
     const size_t es = P->opt.sino == RECON_SINO_BF16 ? 2 : 4;
-    const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * P->npix * es;
+    const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * column_view_elems(*P) * es;
     return exact_bp(*P, r, true, P->opt.sino == RECON_SINO_BF16, first, count, false, false, d_ht, nullptr, nullptr,
                     s);
 }
@@ -595,7 +598,7 @@ recon_status_t recon_osem(recon_plan_t P, const void* d_g, unsigned iters, unsig
         for (unsigned k = 0; k < n_subsets; ++k) {
             const unsigned first = k * n;
             RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, s, first, n));
-            const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * P->npix * es;
+            const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * column_view_elems(*P) * es;
             RB_CHECK(exact_bp(*P, r, true, bf16, first, n, false, false, nullptr,
                               P->d_osem_sens + (size_t)k * P->nvox, d_f, s));
         }

@@ -720,6 +720,253 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_mirror_kernel(
     }
 }
 
+// bp_gather_mirror_kernel reading its values in mirrored row pairs
+// (kLayoutPairs: per detector column, pair p = {row p, row Nv-1-p} for p = 0 ..
+// Nv/2, even Nv): a lower voxel's candidate row a and the mirror row Nv-1-a
+// come in one load.  Lengths, sums and their order are bp_gather_mirror_kernel's,
+// so both give the same bits.
+template <int EPI, class ST, int PS>
+__global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_pairs_kernel(
+    ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
+    const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned view0, unsigned nview,
+    const ST* __restrict__ vals, size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens,
+    unsigned long long* __restrict__ npairs)
+{
+    extern __shared__ float4 szq[];  // as in bp_gather_kernel
+    __shared__ GatherView sview[kGatherWarps][32];
+    __shared__ float sacc2[kGatherWarps][2][PS * 32];  // further candidates: lower voxels, mirrors
+    for (int q = threadIdx.x; q < G.Nv; q += blockDim.x) {
+        const ZParam z = zp[q];
+        const float kc = (float)z.kc;
+        szq[q] = (z.S > 0.0f) ? make_float4(z.S, z.O, kc, kc - 1.0f) : make_float4(z.S, z.O, kc - 1.0f, kc);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = blockIdx.x * kGatherTileX, j0 = blockIdx.y * (kGatherWarps / kGatherTileX);
+    const int i = i0 + warp % kGatherTileX, j = j0 + warp / kGatherTileX;
+    const unsigned nview_w = (i < G.X && j < G.Y) ? nview : 0u;  // as in bp_gather_kernel
+    GatherView* sv = sview[warp];
+    float* acc2 = sacc2[warp][0];
+    float* acc2m = sacc2[warp][1];
+    const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
+    const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
+    const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;  // margins as in bp_gather_kernel
+    const float dz32 = 32.0f * G.vox[2];
+    const int Zh = G.Z / 2;
+    const unsigned top = (unsigned)G.Nv - 1u;
+    const unsigned Nh = (unsigned)G.Nv / 2u, Np = Nh + 1u;  // pairs per detector column
+    for (int k0 = 0; k0 < Zh; k0 += 32 * PS) {
+        const float fk0 = (float)(k0 + lane);
+        const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
+        const int nslot = min(PS, max(0, (Zh - k0 - lane + 31) / 32));
+        float acc[PS], accm[PS];
+#pragma unroll
+        for (int s = 0; s < PS; ++s) {
+            acc[s] = 0.0f;
+            accm[s] = 0.0f;
+            acc2[s * 32 + lane] = 0.0f;
+            acc2m[s * 32 + lane] = 0.0f;
+        }
+        // detector column u of one view: its piece [A, B], row coefficients and
+        // steps; col = the view's values from row 0 of column u
+        auto piece = [&](float A, float B, float ca, float cb, float pa, float pb, bool single, bool behind,
+                         const ST* __restrict__ col) {
+            // row v's length through lower voxel s of this lane
+            auto length = [&](int s, int v) {
+                const float4 zr = szq[v];
+                const float t = fk0 + (float)(32 * s);
+                const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                return fminf(B, hi) - fmaxf(A, lo);
+            };
+            if (behind) {  // a piece behind the source: every row is a candidate
+#pragma unroll
+                for (int s = 0; s < PS; ++s)
+                    if (s < nslot)
+                        for (int v = 0; v < G.Nv; ++v) {
+                            const float L = length(s, v);
+                            if (L > 0.0f) {
+                                // row v and its mirror from pair min(v, Nv-1-v), in order
+                                const bool lower = (unsigned)v < Nh;
+                                const auto p = load_pair_raw(col + 2u * (lower ? (unsigned)v : top - v));
+                                const float xv = lower ? widen_lo(p) : widen_hi(p), xm = lower ? widen_hi(p) : widen_lo(p);
+                                acc[s] = (EPI == 2) ? acc[s] + 1.0f : fmaf(L, xv, acc[s]);
+                                accm[s] = (EPI == 2) ? accm[s] + 1.0f : fmaf(L, xm, accm[s]);
+                            }
+                        }
+                return;
+            }
+            // row bounds of a lower voxel: f0 = its bottom row at the piece's near
+            // end, f1 = its top row at the far end (the voxel lies below z = 0)
+            const float P0a = fmaf(zl0, ca, oz_lo);
+            const float P1b = single ? 0.0f : fmaf(zh0, cb, oz_hi);
+            auto first_rows = [&](auto single_tag) -> unsigned {
+                constexpr bool SINGLE = decltype(single_tag)::value;
+                unsigned more = 0u;
+                int vl[PS];
+                decltype(load_pair_raw(col)) x[PS];
+#pragma unroll
+                for (int s = 0; s < PS; ++s) {
+                    const float f0 = fmaf((float)s, pa, P0a);
+                    // a lower voxel's rows lie at or below row Nv/2 (its z is at or below
+                    // the source plane; the pair table's last entry is row Nv/2): clamped
+                    // there, every load is in bounds, and a row that is no candidate has
+                    // no positive length (see bp_gather_kernel)
+                    const unsigned a = min(__float2uint_ru(f0), Nh);
+                    vl[s] = (int)a;
+                    x[s] = load_pair_raw(col + 2u * a);
+                    if (!SINGLE) {
+                        const float f1 = fmaf((float)s, pb, P1b);
+                        if ((float)(a + 1u) <= f1) more |= 1u << s;
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < PS; ++s) {
+                    const float L = length(s, vl[s]);
+                    if (L > 0.0f) {
+                        acc[s] = (EPI == 2) ? acc[s] + 1.0f : fmaf(L, widen_lo(x[s]), acc[s]);
+                        accm[s] = (EPI == 2) ? accm[s] + 1.0f : fmaf(L, widen_hi(x[s]), accm[s]);
+                    }
+                }
+                return more;
+            };
+            if (single) {
+                first_rows(std::true_type{});
+                return;
+            }
+            const unsigned more = first_rows(std::false_type{});
+            // further candidates (rare): summed apart, in shared memory, over the
+            // bounds of both piece ends as bp_gather_kernel takes them
+            if (__any_sync(0xffffffffu, more != 0u)) {
+                const float P0b = fmaf(zl0, cb, oz_lo), P1a = fmaf(zh0, ca, oz_hi);
+                for (unsigned m = more; m != 0u; m &= m - 1u) {
+                    const int s = __ffs(m) - 1;
+                    const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
+                    const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                    const int a = max(0, __float2int_ru(f0));
+                    const int b = min((int)Nh, __float2int_rd(f1));
+                    float sum = acc2[s * 32 + lane], summ = acc2m[s * 32 + lane];
+                    for (int v = a + 1; v <= b; ++v) {
+                        const float L = length(s, v);
+                        if (L > 0.0f) {
+                            const auto p = load_pair_raw(col + 2 * v);
+                            sum = (EPI == 2) ? sum + 1.0f : fmaf(L, widen_lo(p), sum);
+                            summ = (EPI == 2) ? summ + 1.0f : fmaf(L, widen_hi(p), summ);
+                        }
+                    }
+                    acc2[s * 32 + lane] = sum;
+                    acc2m[s * 32 + lane] = summ;
+                }
+            }
+        };
+        for (unsigned vb = 0; vb < nview_w; vb += 32) {
+            const unsigned nb = min(32u, nview_w - vb);
+            if ((unsigned)lane < nb)  // lane q sets up view vb + q
+                sv[lane] = gather_view(G, C, txy, kxy, cs, view0 + vb + lane, i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo,
+                                       dz32);
+            __syncwarp();
+            for (unsigned q = 0; q < nb; ++q) {
+                const unsigned vi = vb + q;
+                const int ulo = sv[q].u_lo, uhi = sv[q].u_hi;
+                const unsigned fl = sv[q].flags;
+#pragma unroll 1
+                for (int sl = 0; sl < 2; ++sl) {
+                    if (ulo + sl > uhi) break;
+                    if (!((fl >> sl) & 1u)) continue;  // the rays miss the column
+                    const float4 ab = sv[q].ab[sl];
+                    const float2 cc = sv[q].c[sl];
+                    piece(ab.x, ab.y, cc.x, cc.y, ab.z, ab.w, (fl >> (2 + sl)) & 1u, (fl >> (4 + sl)) & 1u,
+                          vals + (size_t)vi * view_stride + (size_t)(ulo + sl) * Np * 2);
+                }
+                // a column wider than two detector pitches: set up here
+                for (int u = ulo + 2; u <= uhi; ++u) {
+                    const unsigned view = view0 + vi;
+                    const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
+                    const int2 K = __ldg(kxy + (size_t)view * G.Nu + u);
+                    const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+                    const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+                    const float A = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                    const float B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+                    if (!(A < B)) continue;
+                    const float ca = C.ez / (A + G.Rf), cb = C.ez / (B + G.Rf);
+                    piece(A, B, ca, cb, dz32 * ca, dz32 * cb, false, !(A + G.Rf > 1e-3f * G.Rf),
+                          vals + (size_t)vi * view_stride + (size_t)u * Np * 2);
+                }
+            }
+            __syncwarp();  // the next batch rewrites sv
+        }
+        if (EPI == 2) {  // pair counts
+            unsigned long long c = 0;
+#pragma unroll
+            for (int s = 0; s < PS; ++s)
+                if (s < nslot)
+                    c += (unsigned long long)(acc[s] + acc2[s * 32 + lane]) +
+                         (unsigned long long)(accm[s] + acc2m[s * 32 + lane]);
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0 && c) atomicAdd(npairs, c);
+        } else {
+            // entries [0, 32 PS) the lower voxels k0 + e, [32 PS, 64 PS) their mirrors
+#pragma unroll
+            for (int s = 0; s < PS; ++s) {
+                acc2[s * 32 + lane] += acc[s];
+                acc2m[s * 32 + lane] += accm[s];
+            }
+            __syncthreads();
+            gather_tile_epilogue<EPI, 64 * PS>(
+                G, C.vec4 != 0, &sacc2[0][0][0], i0, j0,
+                [&](int e) {
+                    const int k = k0 + (e < 32 * PS ? e : e - 32 * PS);
+                    return k >= Zh ? -1 : (e < 32 * PS ? k : G.Z - 1 - k);
+                },
+                vol, sens);
+            __syncthreads();  // the next chunk clears the entries
+        }
+    }
+}
+
+
+// A sinogram [view][v][u] times w into mirrored row pairs (kLayoutPairs), 32 (u)
+// x 32 (pair) tiles: both rows of each pair read along u through shared memory,
+// w (detector columns, wq) and the pairs along the pair index.
+template <class T>
+__global__ void __launch_bounds__(256) to_pairs_kernel(const T* __restrict__ in, const float* __restrict__ wq, int Nu,
+                                                        int Nv, T* __restrict__ out)
+{
+    __shared__ float lo[32][33], hi[32][33];
+    const int Np = Nv / 2 + 1;
+    const int u0 = blockIdx.x * 32, p0 = blockIdx.y * 32;
+    const size_t base = (size_t)blockIdx.z * Nu * Nv;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int u = u0 + threadIdx.x, p = p0 + r;
+        if (u < Nu && p < Np) {
+            lo[r][threadIdx.x] = load_val<T>(in + base + (size_t)p * Nu + u);
+            hi[r][threadIdx.x] = load_val<T>(in + base + (size_t)(Nv - 1 - p) * Nu + u);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int u = u0 + threadIdx.y + 8 * q, p = p0 + threadIdx.x;
+        if (u >= Nu || p >= Np) continue;
+        const float wa = wq ? __ldg(wq + (size_t)u * Nv + p) : 1.0f;
+        const float wb = wq ? __ldg(wq + (size_t)u * Nv + (Nv - 1 - p)) : 1.0f;
+        store_pair<T>(out + (((size_t)blockIdx.z * Nu + u) * Np + p) * 2, lo[threadIdx.x][threadIdx.y + 8 * q] * wa,
+                      hi[threadIdx.x][threadIdx.y + 8 * q] * wb);
+    }
+}
+
+// wq (detector columns [u][v]) into mirrored row pairs.
+__global__ void wq_pairs_kernel(const float* __restrict__ wq, int Nu, int Nv, float* __restrict__ out)
+{
+    const int Np = Nv / 2 + 1;
+    const size_t n = (size_t)Nu * Np;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t u = q / Np;
+        const int p = (int)(q % Np);
+        out[2 * q] = wq[u * Nv + p];
+        out[2 * q + 1] = wq[u * Nv + (Nv - 1 - p)];
+    }
+}
+
 // A sinogram [view][v][u] (times w when w is given) into the detector-column
 // layout [view][u][v] that the gather back projectors read: 32x32 (u, v) tiles
 // through shared memory, read and written along rows of 128 bytes.  With rect
@@ -1129,8 +1376,10 @@ recon_status_t exact_fp_ratio(Plan& P, const float* vol, const void* g, void* ra
     if (P.fp_column) {  // straight into the layout the back projector reads
         const bool bf16 = P.opt.sino == RECON_SINO_BF16;
         const size_t es = bf16 ? sizeof(bf) : sizeof(float);
-        return exact_fp_column_ratio(P, vol, (const char*)g + off * es, (char*)ratio + off * es, 1,
-                                     mlem_ratio_in_columns(P), bf16, first, count, s);
+        const int layout = !mlem_ratio_in_columns(P) ? kLayoutRows : P.col_pairs ? kLayoutPairs : kLayoutColumns;
+        const size_t roff = (size_t)first * (layout == kLayoutPairs ? column_view_elems(P) : P.npix);
+        return exact_fp_column_ratio(P, vol, (const char*)g + off * es, (char*)ratio + roff * es, 1, layout, bf16,
+                                     first, count, s);
     }
     if (P.opt.sino == RECON_SINO_BF16) {
         bf* r = mlem_ratio_in_columns(P) ? (bf*)P.d_ratio_rm : (bf*)ratio;
@@ -1224,7 +1473,9 @@ recon_status_t exact_count(Plan& P, unsigned long long* out)
 
 recon_status_t exact_fp_plain_ratio(Plan& P, const float* vol, const float* g, float* ratio, cudaStream_t s)
 {
-    if (P.fp_column) return exact_fp_column_ratio(P, vol, g, ratio, 2, voxel_ratio_in_columns(P), false, 0u, P.nviews, s);
+    if (P.fp_column)
+        return exact_fp_column_ratio(P, vol, g, ratio, 2, voxel_ratio_in_columns(P) ? kLayoutColumns : kLayoutRows,
+                                     false, 0u, P.nviews, s);
     if (voxel_ratio_in_columns(P)) {
         float* r = (float*)P.d_ratio_rm;
         RB_CHECK((launch_fp<2, float, float>(P, vol, 0u, P.nviews, g, r, s)));
@@ -1411,6 +1662,7 @@ recon_status_t exact_tune_bp(Plan& P)
         recon_status_t st = RECON_OK;
         for (int d = 0; d < 2 && e == cudaSuccess && st == RECON_OK; ++d) {
             P.bp_gather = (d == 0);
+            P.col_pairs = (d == 0) && P.d_wq_pairs != nullptr;  // as the plan will use the gather
             st = exact_bp(P, nullptr, false, false, 0, P.nviews, false, true, out, nullptr, nullptr, 0);
             if (st == RECON_OK) e = cudaEventRecord(e0, 0);
             if (e == cudaSuccess && st == RECON_OK)
@@ -1461,8 +1713,9 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
     C.vec4 = (E.X % 4 == 0) && (reinterpret_cast<uintptr_t>(vol) % 16 == 0) &&
              (reinterpret_cast<uintptr_t>(sens) % 16 == 0);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
-    auto kernel = [] {
-        if constexpr (MIRROR) return exact::bp_gather_mirror_kernel<EPI, ST, SLOTS>;
+    auto kernel = [&P] {
+        if constexpr (MIRROR)
+            return P.col_pairs ? exact::bp_gather_pairs_kernel<EPI, ST, SLOTS> : exact::bp_gather_mirror_kernel<EPI, ST, SLOTS>;
         else return exact::bp_gather_kernel<EPI, ST, SLOTS>;
     }();
     const size_t static_smem = sizeof(exact::GatherView) * 32 * exact::kGatherWarps +          // sview
@@ -1549,11 +1802,11 @@ static recon_status_t ensure_column_scratch(Plan& P, unsigned count)
     if (P.d_colsino) {
         cudaFree(P.d_colsino);
         P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), (void*)P.d_colsino));
-        P.device_bytes -= (size_t)P.colsino_views * P.npix * sizeof(float);
+        P.device_bytes -= (size_t)P.colsino_views * column_view_elems(P) * sizeof(float);
         P.d_colsino = nullptr;
         P.colsino_views = 0;
     }
-    RB_CHECK(P.alloc(&P.d_colsino, (size_t)count * P.npix, "detector-column sinogram"));
+    RB_CHECK(P.alloc(&P.d_colsino, (size_t)count * column_view_elems(P), "detector-column sinogram"));
     P.colsino_views = count;
     return RECON_OK;
 }
@@ -1573,6 +1826,28 @@ bool voxel_ratio_in_columns(const Plan& P)
     return P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_VOXEL && P.opt.voxel_mode == RECON_VOXEL_GEOMETRIC;
 }
 
+// The gather's inputs in mirrored row pairs (kLayoutPairs) where both projectors
+// pair mirrored rows: the z table is mirror-symmetric, the forward projector
+// walks detector columns, the detector has an even row count.  Builds the pair
+// copy of w that the sensitivity reads; the plan sets col_pairs where the
+// gather is its back projector.
+bool exact_pairs_suit(const Plan& P)
+{
+    return P.z_mirror && P.fp_column && P.eg.Nv % 2 == 0 && P.opt.arith == RECON_ARITH_EXACT &&
+           P.opt.bp == RECON_BP_SIDDON;
+}
+
+recon_status_t build_wq_pairs(Plan& P)
+{
+    if (P.d_wq_pairs) return RECON_OK;
+    const size_t n = (size_t)P.eg.Nu * (P.eg.Nv / 2 + 1);
+    RB_CHECK(P.alloc(&P.d_wq_pairs, 2 * n, "ray weights (mirrored row pairs)"));
+    exact::wq_pairs_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 8), 256>>>(P.d_wq, P.eg.Nu, P.eg.Nv,
+                                                                                         P.d_wq_pairs);
+    RB_CUDA(cudaGetLastError());
+    return RECON_OK;
+}
+
 recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, unsigned first, unsigned count,
                         bool scratch_slot, bool sens_mode, float* vol, const float* sens, float* f_update,
                         cudaStream_t s)
@@ -1584,8 +1859,9 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
     if (count == 0) return launch_fill(f_update ? f_update : vol, 0.0f, P.nvox, s);
     using bf = __nv_bfloat16;
     if (P.bp_gather) {
-        const size_t qv = P.npix;
-        if (sens_mode) return launch_gather<false, float>(P, P.d_wq, 0, first, count, vol, nullptr, s);
+        const size_t qv = column_view_elems(P);
+        if (sens_mode)
+            return launch_gather<false, float>(P, P.col_pairs ? P.d_wq_pairs : P.d_wq, 0, first, count, vol, nullptr, s);
         if (sino_is_rw) {  // the MLEM ratio: detector columns, carries w
             float* out = f_update ? f_update : vol;
             if (bf16) {
@@ -1595,9 +1871,16 @@ recon_status_t exact_bp(Plan& P, const void* sino, bool sino_is_rw, bool bf16, u
             if (f_update) return launch_gather<true, float>(P, (const float*)sino, qv, first, count, out, sens, s);
             return launch_gather<false, float>(P, (const float*)sino, qv, first, count, out, nullptr, s);
         }
-        // a sinogram [view][v][u]: weighted by w into the detector-column scratch first
+        // a sinogram [view][v][u]: weighted by w into the gather's layout first
         RB_CHECK(ensure_column_scratch(P, count));
-        RB_CHECK(to_columns<float>(P, (const float*)sino, P.d_w, count, nullptr, P.d_colsino, s));
+        if (P.col_pairs) {
+            const ExactGeom& E = P.eg;
+            exact::to_pairs_kernel<float><<<dim3((E.Nu + 31) / 32, (E.Nv / 2 + 1 + 31) / 32, count), dim3(32, 8), 0, s>>>(
+                (const float*)sino, P.d_wq, E.Nu, E.Nv, P.d_colsino);
+            RB_CUDA(cudaGetLastError());
+        } else {
+            RB_CHECK(to_columns<float>(P, (const float*)sino, P.d_w, count, nullptr, P.d_colsino, s));
+        }
         return launch_gather<false, float>(P, P.d_colsino, qv, first, count, vol, nullptr, s);
     }
     if (sens_mode) return launch_bp<1, false, float>(P, nullptr, first, count, vol, nullptr, s);

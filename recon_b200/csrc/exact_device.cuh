@@ -73,6 +73,31 @@ __device__ __forceinline__ void store_val<float>(float* p, float v) { *p = v; }
 template <>
 __device__ __forceinline__ void store_val<__nv_bfloat16>(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 
+// Two values kept together (mirrored row pairs): one 8-byte access for float,
+// one 4-byte access for bf16; p is aligned to the pair.  load_pair_raw keeps
+// the stored form, widen_lo / widen_hi give the first and second value.
+template <class T>
+__device__ __forceinline__ void store_pair(T* p, float a, float b);
+template <>
+__device__ __forceinline__ void store_pair<float>(float* p, float a, float b)
+{
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+}
+template <>
+__device__ __forceinline__ void store_pair<__nv_bfloat16>(__nv_bfloat16* p, float a, float b)
+{
+    *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+}
+__device__ __forceinline__ float2 load_pair_raw(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+__device__ __forceinline__ unsigned load_pair_raw(const __nv_bfloat16* p)
+{
+    return __ldg(reinterpret_cast<const unsigned*>(p));
+}
+__device__ __forceinline__ float widen_lo(float2 x) { return x.x; }
+__device__ __forceinline__ float widen_hi(float2 x) { return x.y; }
+__device__ __forceinline__ float widen_lo(unsigned x) { return __uint_as_float(x << 16); }
+__device__ __forceinline__ float widen_hi(unsigned x) { return __uint_as_float(x & 0xffff0000u); }
+
 // ---- ray blocks ---------------------------------------------------------------------------
 
 // Rays are launched in blocks of 32 (u) x 4 (v).  A CTA's block comes from a

@@ -329,15 +329,15 @@ __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, cons
 // MODE 5: MODE 3 within one xy block.  MODES 4 and 5 take the column's stretch
 // inside the xy block blk = {x planes blk.x .. blk.y, y planes blk.z .. blk.w},
 // the others the whole volume's.
-// g is read [view][v][u]; out is written in
-// the detector-column layout [view][u][v] when COLS (a warp's 32 rows store
-// 128 contiguous bytes), else [view][v][u].  A CTA takes detector column u of
+// g is read [view][v][u]; out is written in LAYOUT: rows [view][v][u],
+// detector columns [view][u][v] (a warp's 32 rows store 128 contiguous bytes)
+// or, with MIRROR, mirrored row pairs (a lane stores its pair at once).  A CTA takes detector column u of
 // one view and rows vstart .. vstart + kColRows - 1: from the tile list
 // {view, u | vstart << 16} (blockIdx.x indexes it) or, without one, u =
 // blockIdx.x, vstart = blockIdx.y * kColRows, view = view0 + blockIdx.z.
 // MIRROR: rows come in mirrored pairs (see walk_rows_mirror); the CTA's rows
 // are lower rows (below Nv/2) and each lane also produces its mirror row.
-template <bool KAHAN, int MODE, bool COLS, class GT, class OT, bool MIRROR = false>
+template <bool KAHAN, int MODE, int LAYOUT, class GT, class OT, bool MIRROR = false>
 __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                              const int2* __restrict__ kxy,
                                                              const ZParam* __restrict__ zp,
@@ -428,26 +428,35 @@ __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const 
     if (!valid) return;
     if constexpr (!COUNTING) {
         const size_t base = (size_t)(view - view0) * G.Nu * G.Nv;
-        auto emit = [&](int row, float acc) {
+        // row's output value (MODE 0..2)
+        auto value = [&](int row, float acc) {
             const size_t pix_rm = (size_t)row * G.Nu + u, pix_col = (size_t)u * G.Nv + row;
-            if constexpr (MODE == 4) {
-                static_assert(COLS, "block sums are kept in the detector-column layout");
-                out[base + pix_col] += acc;
-            } else {
-                const float w = __ldg(wq + pix_col);
-                const float hf = w * acc;
-                OT* const o = out + base + (COLS ? pix_col : pix_rm);
-                if (MODE == 0) {
-                    store_val<OT>(o, hf);
-                } else {
-                    const float gv = load_val<GT>(g + base + pix_rm);
-                    const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
-                    store_val<OT>(o, MODE == 1 ? ratio * w : ratio);
-                }
-            }
+            const float w = __ldg(wq + pix_col);
+            const float hf = w * acc;
+            if (MODE == 0) return hf;
+            const float gv = load_val<GT>(g + base + pix_rm);
+            const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
+            return MODE == 1 ? ratio * w : ratio;
         };
-        emit(v, sum.x);
-        if (MIRROR) emit(G.Nv - 1 - v, sum.y);
+        if constexpr (MODE == 4) {
+            static_assert(LAYOUT == kLayoutColumns, "block sums are kept in the detector-column layout");
+            out[base + (size_t)u * G.Nv + v] += sum.x;
+            if (MIRROR) out[base + (size_t)u * G.Nv + (G.Nv - 1 - v)] += sum.y;
+        } else if constexpr (LAYOUT == kLayoutPairs) {
+            static_assert(MIRROR, "mirrored row pairs come from the mirror-paired walk");
+            const int Np = G.Nv / 2 + 1;
+            OT* const o = out + ((size_t)(view - view0) * G.Nu + u) * Np * 2;
+            const float a = value(v, sum.x), b = value(G.Nv - 1 - v, sum.y);
+            store_pair<OT>(o + 2 * v, a, b);
+            if (v == G.Nv / 2 - 1) store_pair<OT>(o + 2 * (v + 1), b, a);  // entry Nv/2: rows Nv/2, Nv/2 - 1
+        } else {
+            auto emit = [&](int row, float acc) {
+                const size_t pix = LAYOUT == kLayoutColumns ? (size_t)u * G.Nv + row : (size_t)row * G.Nu + u;
+                store_val<OT>(out + base + pix, value(row, acc));
+            };
+            emit(v, sum.x);
+            if (MIRROR) emit(G.Nv - 1 - v, sum.y);
+        }
     }
 }
 
@@ -498,7 +507,7 @@ __global__ void __launch_bounds__(128) column_block_mask_kernel(ExactGeom G, con
 // 32 (u) x 32 (v) tiles: g is read along u and acc, w along v; a row-major out
 // is written along u through the same tile.  acc may be out itself (float,
 // detector-column layout): each thread reads its pixel before writing it.
-template <int MODE, bool COLS, class GT, class OT>
+template <int MODE, int LAYOUT, class GT, class OT>
 __global__ void __launch_bounds__(256) column_finish_kernel(ExactGeom G, const float* acc,
                                                             const float* __restrict__ wq,
                                                             const GT* __restrict__ g, OT* out)
@@ -528,10 +537,10 @@ __global__ void __launch_bounds__(256) column_finish_kernel(ExactGeom G, const f
                 const float ratio = (hf != 0.0f) ? __fdiv_rn(tile[threadIdx.x][threadIdx.y + 8 * q], hf) : 0.0f;
                 val[q] = MODE == 1 ? ratio * w : ratio;
             }
-            if (COLS) store_val<OT>(out + base + pc, val[q]);
+            if (LAYOUT == kLayoutColumns) store_val<OT>(out + base + pc, val[q]);
         }
     }
-    if (!COLS) {
+    if (LAYOUT == kLayoutRows) {
         __syncthreads();  // the g tile is read
 #pragma unroll
         for (int q = 0; q < 4; ++q) tile[threadIdx.x][threadIdx.y + 8 * q] = val[q];
@@ -540,6 +549,47 @@ __global__ void __launch_bounds__(256) column_finish_kernel(ExactGeom G, const f
             const int u = u0 + threadIdx.x, v = v0 + r;
             if (u < G.Nu && v < G.Nv) store_val<OT>(out + base + (size_t)v * G.Nu + u, tile[r][threadIdx.x]);
         }
+    }
+}
+
+// column_finish_kernel for an output in mirrored row pairs: 32 (u) x 32 (pair)
+// tiles, g of both rows of each pair read along u through shared memory, acc
+// and w read along the pair index (rows p ascending, rows Nv-1-p descending),
+// each pair stored at once.
+template <int MODE, class GT, class OT>
+__global__ void __launch_bounds__(256) column_finish_pairs_kernel(ExactGeom G, const float* __restrict__ acc,
+                                                                  const float* __restrict__ wq,
+                                                                  const GT* __restrict__ g, OT* __restrict__ out)
+{
+    __shared__ float lo[32][33], hi[32][33];
+    const int Np = G.Nv / 2 + 1;
+    const int u0 = blockIdx.x * 32, p0 = blockIdx.y * 32;
+    const size_t base = (size_t)blockIdx.z * G.Nu * G.Nv;
+    if (MODE != 0) {
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int u = u0 + threadIdx.x, p = p0 + r;
+            if (u < G.Nu && p < Np) {
+                lo[r][threadIdx.x] = load_val<GT>(g + base + (size_t)p * G.Nu + u);
+                hi[r][threadIdx.x] = load_val<GT>(g + base + (size_t)(G.Nv - 1 - p) * G.Nu + u);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int u = u0 + threadIdx.y + 8 * q, p = p0 + threadIdx.x;
+        if (u >= G.Nu || p >= Np) continue;
+        auto value = [&](int row, float gv) {
+            const size_t pc = (size_t)u * G.Nv + row;
+            const float w = __ldg(wq + pc);
+            const float hf = w * acc[base + pc];
+            if (MODE == 0) return hf;
+            const float ratio = (hf != 0.0f) ? __fdiv_rn(gv, hf) : 0.0f;
+            return MODE == 1 ? ratio * w : ratio;
+        };
+        const float a = value(p, MODE ? lo[threadIdx.x][threadIdx.y + 8 * q] : 0.0f);
+        const float b = value(G.Nv - 1 - p, MODE ? hi[threadIdx.x][threadIdx.y + 8 * q] : 0.0f);
+        store_pair<OT>(out + (((size_t)blockIdx.z * G.Nu + u) * Np + p) * 2, a, b);
     }
 }
 
@@ -682,15 +732,19 @@ recon_status_t exact_to_zfast(const Plan& P, const float* vol, cudaStream_t s)
 // volume is copied to the z-fastest layout first.  For MODE 0 the pixels
 // outside the tiles are zeroed; the MLEM ratio buffers are zero there from
 // allocation on.
-template <int MODE, bool COLS, class GT, class OT>
+template <int MODE, int LAYOUT, class GT, class OT>
 static auto column_kernel(const Plan& P)
 {
     const bool kahan = P.opt.sum == RECON_SUM_KAHAN;
-    auto kernel = P.z_mirror ? (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, true>
-                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, true>)
-                             : (kahan ? exact::fp_column_kernel<true, MODE, COLS, GT, OT, false>
-                                      : exact::fp_column_kernel<false, MODE, COLS, GT, OT, false>);
-    return kernel;
+    if constexpr (LAYOUT == kLayoutPairs) {  // only from the mirror-paired walk
+        return kahan ? exact::fp_column_kernel<true, MODE, LAYOUT, GT, OT, true>
+                     : exact::fp_column_kernel<false, MODE, LAYOUT, GT, OT, true>;
+    } else {
+        return P.z_mirror ? (kahan ? exact::fp_column_kernel<true, MODE, LAYOUT, GT, OT, true>
+                                   : exact::fp_column_kernel<false, MODE, LAYOUT, GT, OT, true>)
+                          : (kahan ? exact::fp_column_kernel<true, MODE, LAYOUT, GT, OT, false>
+                                   : exact::fp_column_kernel<false, MODE, LAYOUT, GT, OT, false>);
+    }
 }
 
 // Views [first, first + count) of plan views over the xy blocks: each block's
@@ -698,13 +752,13 @@ static auto column_kernel(const Plan& P)
 // are deterministic), then column_finish_kernel forms the output; MODE 3 adds
 // each block's pair count.  acc is the output itself where that is float in
 // detector columns, else the plan's block-sum buffer.
-template <int MODE, bool COLS, class GT, class OT>
+template <int MODE, int LAYOUT, class GT, class OT>
 static recon_status_t launch_column_blocks(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g,
                                           OT* out, cudaStream_t s)
 {
     const ExactGeom& E = P.eg;
     const size_t smem = (size_t)(E.X + E.Y + 2) * sizeof(float2);
-    constexpr bool in_place = COLS && std::is_same<OT, float>::value;
+    constexpr bool in_place = LAYOUT == kLayoutColumns && std::is_same<OT, float>::value;
     float* acc = nullptr;
     if (MODE != 3) {
         if (in_place) {
@@ -718,7 +772,7 @@ static recon_status_t launch_column_blocks(Plan& P, const float* vol, unsigned f
     }
     constexpr int BMODE = MODE == 3 ? 5 : 4;
     using BOT = typename std::conditional<MODE == 3, OT, float>::type;
-    auto kernel = column_kernel<BMODE, MODE == 3 ? COLS : true, float, BOT>(P);
+    auto kernel = column_kernel<BMODE, MODE == 3 ? LAYOUT : kLayoutColumns, float, BOT>(P);
     if (smem > 48 * 1024) RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     BOT* bout;
     if constexpr (MODE == 3) bout = out;
@@ -735,9 +789,13 @@ static recon_status_t launch_column_blocks(Plan& P, const float* vol, unsigned f
                                                      P.d_vol_z, nullptr, bout);
             RB_CUDA(cudaGetLastError());
         }
-    if constexpr (MODE != 3) {
+    if constexpr (MODE != 3 && LAYOUT == kLayoutPairs) {
+        const dim3 grid((E.Nu + 31) / 32, (E.Nv / 2 + 1 + 31) / 32, count);
+        exact::column_finish_pairs_kernel<MODE, GT, OT><<<grid, dim3(32, 8), 0, s>>>(E, acc, P.d_wq, g, out);
+        RB_CUDA(cudaGetLastError());
+    } else if constexpr (MODE != 3) {
         const dim3 grid((E.Nu + 31) / 32, (E.Nv + 31) / 32, count);
-        exact::column_finish_kernel<MODE, COLS, GT, OT><<<grid, dim3(32, 8), 0, s>>>(E, acc, P.d_wq, g, out);
+        exact::column_finish_kernel<MODE, LAYOUT, GT, OT><<<grid, dim3(32, 8), 0, s>>>(E, acc, P.d_wq, g, out);
         RB_CUDA(cudaGetLastError());
     }
     return RECON_OK;
@@ -748,7 +806,7 @@ static recon_status_t launch_column_blocks(Plan& P, const float* vol, unsigned f
 // volume is copied to the z-fastest layout first.  For MODE 0 the pixels
 // outside the tiles are zeroed; the MLEM ratio buffers are zero there from
 // allocation on.  Plans with xy blocks take plan views block by block.
-template <int MODE, bool COLS, class GT, class OT>
+template <int MODE, int LAYOUT, class GT, class OT>
 static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, unsigned count, const GT* g, OT* out,
                                     cudaStream_t s)
 {
@@ -756,7 +814,7 @@ static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, u
     const ExactGeom& E = P.eg;
     const bool plan_views = first + count <= P.nviews;
     if (plan_views && P.col_block > 0 && P.col_btiles.size() == (size_t)P.col_nbx * P.col_nby)
-        return launch_column_blocks<MODE, COLS, GT, OT>(P, vol, first, count, g, out, s);
+        return launch_column_blocks<MODE, LAYOUT, GT, OT>(P, vol, first, count, g, out, s);
     dim3 grid;
     const uint2* tiles = nullptr;
     if (plan_views && P.col_tiles.prefix.size() == P.nviews + 1) {
@@ -771,7 +829,7 @@ static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, u
     }
     if (MODE != 3) RB_CHECK(exact_to_zfast(P, vol, s));
     const size_t smem = (size_t)(E.X + E.Y + 2) * sizeof(float2);
-    auto kernel = column_kernel<MODE, COLS, GT, OT>(P);
+    auto kernel = column_kernel<MODE, LAYOUT, GT, OT>(P);
     if (smem > 48 * 1024) RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kernel<<<grid, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, tiles, first,
                                                make_int4(0, E.X, 0, E.Y), P.d_vol_z, g, out);
@@ -787,7 +845,8 @@ recon_status_t exact_fp_column_count(Plan& P, unsigned long long* total)
     RB_CUDA(cudaMalloc(&d, sizeof(unsigned long long)));
     cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
     recon_status_t st = RECON_OK;
-    if (e == cudaSuccess) st = launch_column<3, false, float, unsigned long long>(P, nullptr, 0u, P.nviews, nullptr, d, 0);
+    if (e == cudaSuccess)
+        st = launch_column<3, kLayoutRows, float, unsigned long long>(P, nullptr, 0u, P.nviews, nullptr, d, 0);
     if (e == cudaSuccess && st == RECON_OK) e = cudaMemcpy(total, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (st != RECON_OK) return st;
@@ -797,26 +856,33 @@ recon_status_t exact_fp_column_count(Plan& P, unsigned long long* total)
 
 recon_status_t exact_fp_column(Plan& P, const float* vol, unsigned first, unsigned count, float* out, cudaStream_t s)
 {
-    return launch_column<0, false, float, float>(P, vol, first, count, nullptr, out, s);
+    return launch_column<0, kLayoutRows, float, float>(P, vol, first, count, nullptr, out, s);
 }
 
 // The MLEM ratio (MODE 1: times w, Siddon back projectors; MODE 2: without w,
 // voxel-driven) of views [first, first+count), written straight into the
-// layout its back projector reads.  g and ratio start at view `first`.
-recon_status_t exact_fp_column_ratio(Plan& P, const float* vol, const void* g, void* ratio, int mode, bool cols,
+// layout its back projector reads (kLayoutRows, kLayoutColumns or, for MODE 1,
+// kLayoutPairs).  g and ratio start at view `first`.
+recon_status_t exact_fp_column_ratio(Plan& P, const float* vol, const void* g, void* ratio, int mode, int layout,
                                      bool bf16, unsigned first, unsigned count, cudaStream_t s)
 {
     using bf = __nv_bfloat16;
+    const float* gf = static_cast<const float*>(g);
+    float* rf = static_cast<float*>(ratio);
     if (mode == 2) {
-        if (cols) return launch_column<2, true, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
-        return launch_column<2, false, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
+        if (layout == kLayoutColumns) return launch_column<2, kLayoutColumns, float, float>(P, vol, first, count, gf, rf, s);
+        return launch_column<2, kLayoutRows, float, float>(P, vol, first, count, gf, rf, s);
     }
     if (bf16) {
-        if (cols) return launch_column<1, true, bf, bf>(P, vol, first, count, (const bf*)g, (bf*)ratio, s);
-        return launch_column<1, false, bf, bf>(P, vol, first, count, (const bf*)g, (bf*)ratio, s);
+        const bf* gb = static_cast<const bf*>(g);
+        bf* rb = static_cast<bf*>(ratio);
+        if (layout == kLayoutPairs) return launch_column<1, kLayoutPairs, bf, bf>(P, vol, first, count, gb, rb, s);
+        if (layout == kLayoutColumns) return launch_column<1, kLayoutColumns, bf, bf>(P, vol, first, count, gb, rb, s);
+        return launch_column<1, kLayoutRows, bf, bf>(P, vol, first, count, gb, rb, s);
     }
-    if (cols) return launch_column<1, true, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
-    return launch_column<1, false, float, float>(P, vol, first, count, (const float*)g, (float*)ratio, s);
+    if (layout == kLayoutPairs) return launch_column<1, kLayoutPairs, float, float>(P, vol, first, count, gf, rf, s);
+    if (layout == kLayoutColumns) return launch_column<1, kLayoutColumns, float, float>(P, vol, first, count, gf, rf, s);
+    return launch_column<1, kLayoutRows, float, float>(P, vol, first, count, gf, rf, s);
 }
 
 }  // namespace rb

@@ -78,6 +78,12 @@ struct DeviceBuf {
 // Blocks of 32 x 4 rays that can cross a box of the volume: tiles
 // {view, tu | tv << 16} in view order, prefix[n] = index of view n's first
 // tile (prefix has nviews + 1 entries).
+// Layouts of a sinogram on the device: rows [view][v][u] (the reference's),
+// detector columns [view][u][v], or mirrored row pairs [view][u][p][2] holding
+// {row p, row Nv-1-p} for p = 0 .. Nv/2 (even Nv; entry Nv/2 repeats the last
+// pair swapped), which the mirror-paired gather reads with one load per pair.
+enum : int { kLayoutRows = 0, kLayoutColumns = 1, kLayoutPairs = 2 };
+
 struct RayTiles {
     uint2* d = nullptr;
     std::vector<unsigned> prefix;
@@ -132,6 +138,8 @@ struct Plan {
     // column forward projector over xy blocks (volumes larger than L2): block
     // side in voxels (0: one pass over the whole volume), the blocks' tiles,
     // and block sums [nviews][u][v] where the output cannot hold them
+    bool col_pairs = false;        // the gather's inputs in mirrored row pairs (kLayoutPairs)
+    float* d_wq_pairs = nullptr;   // d_wq in mirrored row pairs (the sensitivity's input)
     int col_block = 0;
     int col_nbx = 1, col_nby = 1;
     std::vector<RayTiles> col_btiles;
@@ -179,6 +187,14 @@ recon_status_t Plan::alloc(T** p, size_t count, const char* what)
     device_bytes += count * sizeof(T);
     *p = static_cast<T*>(q);
     return RECON_OK;
+}
+
+// Elements one view of the gather's input occupies: Nu*Nv in detector columns,
+// Nu*(Nv/2 + 1)*2 in mirrored row pairs.
+inline size_t column_view_elems(const Plan& P)
+{
+    if (!P.col_pairs) return P.npix;
+    return (size_t)P.geom.det.NumAxPixels * (P.geom.det.NumTAxPixels / 2 + 1) * 2;
 }
 
 // ---- entry points implemented in the .cu files --------------------------------
@@ -238,9 +254,11 @@ recon_status_t exact_check_mirror(Plan& P);
 recon_status_t exact_tune_bp(Plan& P);
 // forward projection by detector columns (fpcol.cu)
 bool exact_fp_column_suits(const Plan& P);
+bool exact_pairs_suit(const Plan& P);
+recon_status_t build_wq_pairs(Plan& P);
 recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect);
 recon_status_t exact_fp_column(Plan& P, const float* vol, unsigned first, unsigned count, float* out, cudaStream_t s);
-recon_status_t exact_fp_column_ratio(Plan& P, const float* vol, const void* g, void* ratio, int mode, bool cols,
+recon_status_t exact_fp_column_ratio(Plan& P, const float* vol, const void* g, void* ratio, int mode, int layout,
                                      bool bf16, unsigned first, unsigned count, cudaStream_t s);
 
 recon_status_t launch_elementwise(int op, float* a, const float* b, size_t n, cudaStream_t s);
