@@ -590,7 +590,8 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from recon_b200 import FP_COLUMNS, SIDDON_BP_GATHER, SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN, Options, Plan
+    from recon_b200 import (FP_COLUMN_BLOCKS, FP_COLUMNS, SIDDON_BP_GATHER, SINO_BF16, SINO_F32, SUM_KAHAN, SUM_PLAIN,
+                            Options, Plan)
     from recon_b200.configs import PLAIN_GPU
     from recon_b200.sharding import sharded_mlem_iteration, view_range
 
@@ -637,7 +638,7 @@ def main():
     # (ray + finish) per z-slab (both int64 accumulators of a slab in 64 MiB);
     # at N > 1 a separate update
     gather = P.siddon_bp == SIDDON_BP_GATHER
-    columns = P.forward_projector == FP_COLUMNS
+    columns = P.forward_projector in (FP_COLUMNS, FP_COLUMN_BLOCKS)
     mirror = P.mirror_pairs
     Z, Y, X = P.shape_vol
     depth = max(1, min(Z, (64 << 20) // (X * Y * 16)))
@@ -770,6 +771,8 @@ def main():
         "gpu_launches": args.steps * (2 + bp_launches + (0 if world == 1 else 1)),
         "back_projector": "gather" if gather else "ray",
         "forward_projector": "detector columns" if columns else "ray walk",
+        "ratio_layout": ("mirrored row pairs" if gather and mirror and columns and P.nv % 2 == 0 else
+                         "detector columns" if gather else "rows"),
         "mirror_pairs": mirror,
     }
     peaks = {}
@@ -786,7 +789,11 @@ def main():
         bytes_bp = 4.0 * isects + 12.0 * nvox
         traffic = measured_traffic()
         if t_bp >= t_fp:
-            dom = (("back projection (bp_gather_mirror_kernel)" if mirror else "back projection (bp_gather_kernel)")
+            # mirrored row pairs where both projectors pair rows (even detector height,
+            # detector-column forward projector)
+            pairs = mirror and columns and P.nv % 2 == 0
+            dom = (("back projection (bp_gather_pairs_kernel)" if pairs else
+                    "back projection (bp_gather_mirror_kernel)" if mirror else "back projection (bp_gather_kernel)")
                    if gather else
                    "back projection (maxabs + bp_ray_kernel per z-slab + bp_finish_kernel)", t_bp, bytes_bp,
                    traffic.get("bp"))
