@@ -53,6 +53,7 @@ COUNT_GEOMS = {
     "rows_apart": small_cfg(TAxPixDim=2.0, TAxPixels=36),
     "z256": small_cfg(Xdim=16, Ydim=16, Zdim=256, ZVoxSize=0.25, TAxPixDim=0.5, TAxPixels=160, NumProj=6),
     "cpu_small": scaled(CPU_SMALL, NumProj=30),
+    "thin_ray_walk": small_cfg(ZVoxSize=0.1, TAxPixels=200, TAxPixDim=1.5),
 }
 
 

@@ -39,6 +39,9 @@ GEOMS = {
     # cover 1, 2 and, in TALL below, 7)
     "z100": small_cfg(Zdim=100, TAxPixels=110, NumProj=8),
     "z256": small_cfg(Xdim=16, Ydim=16, Zdim=256, ZVoxSize=0.25, TAxPixDim=0.5, TAxPixels=160, NumProj=6),
+    # a thin slab under steep rows: the ray-walk forward projector with mirrored rows, so the
+    # mirror-paired gather reads the detector-column layout (not row pairs)
+    "thin_ray_walk": small_cfg(ZVoxSize=0.1, TAxPixels=200, TAxPixDim=1.5),
 }
 DESIGNS = {"gather": SIDDON_BP_GATHER, "ray": SIDDON_BP_RAY}
 

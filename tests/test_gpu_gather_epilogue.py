@@ -6,9 +6,10 @@ one float4 per (plane, row) when the width is a multiple of 4 and the image and
 sensitivity are 16-byte aligned, one voxel per thread otherwise.
 recon_mlem_backward over all views (the same sums, written as Ht) followed by
 recon_mlem_update (update_kernel) must give the same image bit for bit.
-Geometries: mirrored voxel pairs and plain, one and several z chunks, widths
-that are and are not multiples of 4, a partial tile row (odd height in y), and
-an image 4 bytes off a 16-byte boundary.
+Geometries: mirrored voxel pairs (ratio in mirrored row pairs, or in detector
+columns behind the ray-walk forward projector) and plain, one and several z
+chunks, widths that are and are not multiples of 4, a partial tile row (odd
+height in y), and an image 4 bytes off a 16-byte boundary.
 """
 import pytest
 
@@ -32,6 +33,8 @@ CASES = {
                                     NumProj=6), True),
     "plain_two_chunks": (small_cfg(Xdim=16, Ydim=18, Zdim=301, ZVoxSize=0.25, TAxPixDim=0.5, TAxPixels=200,
                                    NumProj=6), False),
+    # the ray-walk forward projector: the mirror-paired gather on the detector-column layout
+    "mirror_columns_layout": (small_cfg(ZVoxSize=0.1, TAxPixels=200, TAxPixDim=1.5), True),
 }
 
 
