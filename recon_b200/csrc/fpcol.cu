@@ -331,10 +331,11 @@ __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, cons
 // the others the whole volume's.
 // g is read [view][v][u]; out is written in LAYOUT: rows [view][v][u],
 // detector columns [view][u][v] (a warp's 32 rows store 128 contiguous bytes)
-// or, with MIRROR, mirrored row pairs (a lane stores its pair at once).  A CTA takes detector column u of
-// one view and rows vstart .. vstart + kColRows - 1: from the tile list
-// {view, u | vstart << 16} (blockIdx.x indexes it) or, without one, u =
-// blockIdx.x, vstart = blockIdx.y * kColRows, view = view0 + blockIdx.z.
+// or, with MIRROR, mirrored row pairs (a lane stores its pair at once).  A CTA
+// takes detector column u of one view and rows vstart .. vstart + kColRows - 1:
+// from the tile list {view, u | vstart << 16} (blockIdx.x indexes it) or,
+// without one, u = blockIdx.x, vstart = blockIdx.y * kColRows, view = view0 +
+// blockIdx.z.
 // MIRROR: rows come in mirrored pairs (see walk_rows_mirror); the CTA's rows
 // are lower rows (below Nv/2) and each lane also produces its mirror row.
 template <bool KAHAN, int MODE, int LAYOUT, class GT, class OT, bool MIRROR = false>
