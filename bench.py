@@ -300,6 +300,7 @@ def batched_leg(device, n_prob: int, iters: int, opts, rank: int = 0, world: int
         "speedup": t_plain / t_batch, "batched_isects_per_s": 2.0 * isects * iters / t_batch,
         "plain_isects_per_s": 2.0 * isects * iters / t_plain, "bitwise_equal": bool(same),
         "back_projectors": {"gather": n_gather, "ray": len(plans) - n_gather, "choice": "measured per geometry"},
+        "forward_rows_per_cta": {str(r): sum(1 for P in plans if P.column_rows == r) for r in (0, 32, 64, 128)},
         "alone": {"serial_iter_s": len(plans) / alone_s, "isects_per_s": 2.0 * isects / alone_s, "by_work": bins,
                   "note": "each problem's forward step and back projection timed alone on this rank"},
         "sharding": f"problems by rank over {world} GPUs" if world > 1 else "single GPU",

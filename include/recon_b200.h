@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define RECON_B200_ABI_VERSION 3
+#define RECON_B200_ABI_VERSION 4
 
 typedef enum {
     RECON_OK = 0,
@@ -124,10 +124,12 @@ typedef enum { RECON_VOXEL_REFERENCE = 0, RECON_VOXEL_GEOMETRIC = 1 } recon_voxe
  *     column spans less than a voxel of z, the volume is at least 128 voxels
  *     tall and the detector has at most 3072 rows; RAY otherwise.
  *   TUNED  -- measured: plan creation times a back projection with each
- *     design on the plan's own geometry and keeps the faster.  The choice is
- *     kept for the process per geometry and device, so every plan of that
- *     geometry (a batch's and a plain one alike) makes the same choice and
- *     gives the same bits.  recon_plan_siddon_bp reports it. */
+ *     design on the plan's own geometry and keeps the faster, and times the
+ *     detector-column forward projector with 32, 64 and 128 detector rows per
+ *     CTA and keeps the fastest.  The choices are kept for the process per
+ *     geometry and device, so every plan of that geometry (a batch's and a
+ *     plain one alike) makes the same choices and gives the same bits.
+ *     recon_plan_siddon_bp and recon_plan_column_rows report them. */
 typedef enum {
     RECON_SIDDON_BP_AUTO = 0,
     RECON_SIDDON_BP_GATHER = 1,
@@ -150,6 +152,11 @@ typedef struct {
                      * 40 MiB, so the views in flight reuse it from L2), -1 =
                      * never, n > 0 = n.  Same lengths; the ray sums add the
                      * blocks' shares in block order. */
+    int fp_rows;    /* detector rows per CTA of the detector-column forward
+                     * projector: 0 = AUTO (the fewest of 32, 64, 128 that
+                     * cover a column's rows; measured with
+                     * RECON_SIDDON_BP_TUNED), or 32, 64 or 128.  Results do not
+                     * depend on it. */
 } recon_options_t;
 
 typedef struct recon_plan* recon_plan_t;
@@ -204,6 +211,11 @@ recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design);
  * (no vertical detector offset Dz).  Results are the same either way.  No
  * counterpart in the reference. */
 recon_status_t recon_plan_mirror_pairs(recon_plan_t plan, int* paired);
+/* *rows = the detector rows per CTA of the plan's detector-column forward
+ * projector (32, 64 or 128: the fewest that cover a column's rows, or the
+ * fastest measured with RECON_SIDDON_BP_TUNED), 0 for other forward
+ * projectors.  No counterpart in the reference. */
+recon_status_t recon_plan_column_rows(recon_plan_t plan, int* rows);
 
 /* ---- projectors (device pointers, asynchronous on `stream`) ----------- */
 

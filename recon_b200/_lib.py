@@ -30,7 +30,7 @@ PROJECTOR_BACK = 1  # RECON_PROJECTOR_BACK
 FP_RAY_WALK = 0  # RECON_FP_RAY_WALK
 FP_COLUMNS = 1  # RECON_FP_COLUMNS
 FP_COLUMN_BLOCKS = 2  # RECON_FP_COLUMN_BLOCKS
-ABI_VERSION = 3  # RECON_B200_ABI_VERSION: the layout of the structures above
+ABI_VERSION = 4  # RECON_B200_ABI_VERSION: the layout of the structures above
 
 
 class ReconError(RuntimeError):
@@ -72,7 +72,8 @@ class FilePaths(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("arith", C.c_int), ("sum", C.c_int), ("sino", C.c_int), ("bp", C.c_int),
-                ("voxel_mode", C.c_int), ("device", C.c_int), ("siddon_bp", C.c_int), ("fp_block", C.c_int)]
+                ("voxel_mode", C.c_int), ("device", C.c_int), ("siddon_bp", C.c_int), ("fp_block", C.c_int),
+                ("fp_rows", C.c_int)]
 
 
 _lib = None
@@ -104,6 +105,7 @@ def lib() -> C.CDLL:
         "recon_plan_siddon_bp": (st, [P, ip]),
         "recon_plan_forward_projector": (st, [P, C.POINTER(C.c_int)]),
         "recon_plan_mirror_pairs": (st, [P, C.POINTER(C.c_int)]),
+        "recon_plan_column_rows": (st, [P, C.POINTER(C.c_int)]),
         "recon_march_fp_view": (st, [P, P, f, C.c_int, P, P]),
         "recon_fp_view": (st, [P, P, f, P, P]),
         "recon_fp_views": (st, [P, P, u, u, P, P]),
@@ -151,7 +153,7 @@ def exported_symbols() -> list[str]:
     """Names of the C ABI functions this binding expects (all of include/recon_b200.h)."""
     return [
         "recon_abi_version", "recon_last_error", "recon_default_options", "recon_geometry_from_cfg",
-        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_plan_mirror_pairs", "recon_fp_view", "recon_fp_views",
+        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_plan_mirror_pairs", "recon_plan_column_rows", "recon_fp_view", "recon_fp_views",
         "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_march_fp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_count_projector_pairs", "recon_set_ones", "recon_divide1", "recon_multiply1",

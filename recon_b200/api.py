@@ -28,10 +28,11 @@ class Options:
     device: int = 0
     siddon_bp: int = L.SIDDON_BP_AUTO
     fp_block: int = 0
+    fp_rows: int = 0
 
     def c(self) -> L.Options:
         return L.Options(self.arith, self.sum, self.sino, self.bp, self.voxel_mode, self.device, self.siddon_bp,
-                         self.fp_block)
+                         self.fp_block, self.fp_rows)
 
 
 def geometry(cfg: dict) -> L.Geometry:
@@ -133,6 +134,13 @@ class Plan:
         """The Siddon back projector of an EXACT plan: SIDDON_BP_GATHER or SIDDON_BP_RAY."""
         d = C.c_int(-1)
         check(lib().recon_plan_siddon_bp(self._h, C.byref(d)))
+        return int(d.value)
+
+    @property
+    def column_rows(self) -> int:
+        """recon_plan_column_rows: detector rows per CTA of the column forward projector (0: another)."""
+        d = C.c_int()
+        check(lib().recon_plan_column_rows(self._h, C.byref(d)))
         return int(d.value)
 
     @property

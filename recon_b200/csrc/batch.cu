@@ -195,7 +195,7 @@ recon_status_t recon_batch_create(const recon_geometry_t* geoms, int n, const re
     std::unique_ptr<recon_batch> b(new recon_batch());
     b->device = opt.device;
     std::string key = std::to_string(n) + (opt.sum == RECON_SUM_KAHAN ? "k" : "p") + std::to_string(opt.siddon_bp) +
-                      "b" + std::to_string(opt.fp_block);
+                      "b" + std::to_string(opt.fp_block) + "r" + std::to_string(opt.fp_rows);
     for (int p = 0; p < n; ++p) {
         if (geoms[p].scan.NumProj == 0) return fail(RECON_ERR_INVALID_ARGUMENT, "every problem needs views");
         recon_plan_t plan = nullptr;

@@ -75,6 +75,8 @@ static recon_status_t validate(const recon_geometry_t& g, const recon_options_t&
         o.siddon_bp != RECON_SIDDON_BP_RAY && o.siddon_bp != RECON_SIDDON_BP_TUNED)
         return fail(RECON_ERR_INVALID_ARGUMENT, "unknown siddon_bp option");
     if (o.fp_block < -1) return fail(RECON_ERR_INVALID_ARGUMENT, "fp_block must be -1, 0 or a block side");
+    if (o.fp_rows != 0 && o.fp_rows != 32 && o.fp_rows != 64 && o.fp_rows != 128)
+        return fail(RECON_ERR_INVALID_ARGUMENT, "fp_rows must be 0, 32, 64 or 128");
     if (o.fp_block > 0 && ((v.Xdim + o.fp_block - 1) / o.fp_block) * ((v.Ydim + o.fp_block - 1) / o.fp_block) > 64)
         return fail(RECON_ERR_INVALID_ARGUMENT, "fp_block: more than 64 xy blocks");
     if (o.arith == RECON_ARITH_EXACT) {
@@ -243,6 +245,7 @@ recon_status_t recon_default_options(recon_options_t* opt)
     opt->device = 0;
     opt->siddon_bp = RECON_SIDDON_BP_AUTO;
     opt->fp_block = 0;
+    opt->fp_rows = 0;
     return RECON_OK;
 }
 
@@ -320,6 +323,7 @@ recon_status_t recon_plan_create(const recon_geometry_t* geom, const recon_optio
             if (pairs) RB_CHECK(build_wq_pairs(*P));
             if (tuned) RB_CHECK(exact_tune_bp(*P));
             P->col_pairs = pairs && P->bp_gather;
+            if (tuned && opt.fp_rows == 0) RB_CHECK(exact_tune_fp(*P));
         } else {
             RB_CHECK(P->alloc(&P->d_maxabs, nv1 + 1, "maxabs"));  // per view, scratch slot, all views
             RB_CHECK(P->alloc(&P->d_fix, P->nvox, "fixed-point accumulator"));
@@ -351,6 +355,13 @@ recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design)
     if (plan->opt.arith != RECON_ARITH_EXACT)
         return fail(RECON_ERR_UNSUPPORTED, "COMPAT plans have a single forward projector");
     *design = !plan->fp_column ? RECON_FP_RAY_WALK : plan->col_block > 0 ? RECON_FP_COLUMN_BLOCKS : RECON_FP_COLUMNS;
+    return RECON_OK;
+}
+
+recon_status_t recon_plan_column_rows(recon_plan_t plan, int* rows)
+{
+    if (!plan || !rows) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    *rows = (plan->opt.arith == RECON_ARITH_EXACT && plan->fp_column) ? plan->col_rows : 0;
     return RECON_OK;
 }
 

@@ -1273,7 +1273,11 @@ recon_status_t build_exact_culling(Plan& P)
             P.sino_v1 = std::max(P.sino_v1, r.w);
         }
     P.sino_rows_known = true;
-    if (P.fp_column && P.nviews) RB_CHECK(build_column_tiles(P, rect));
+    P.view_rect_host = rect;
+    if (P.fp_column && P.nviews) {
+        P.col_rows = P.opt.fp_rows ? P.opt.fp_rows : exact_column_rows_default(P, rect);
+        RB_CHECK(build_column_tiles(P, rect));
+    }
     P.bp_tiles.clear();
     if (P.bp_gather) return RECON_OK;  // the gather back projector needs no ray blocks
     const int depth = bp_slab_depth(P);
@@ -1615,8 +1619,11 @@ recon_status_t exact_check_mirror(Plan& P)
 namespace {
 std::mutex g_bp_tune_mutex;
 std::map<std::string, bool> g_bp_tune_gather;
+}  // namespace
 
-std::string bp_tune_key(const Plan& P)
+// The geometry and device of a plan as a key of the tuning caches (floats
+// written exactly, as hexadecimal).
+std::string geometry_key(const Plan& P)
 {
     const recon_geometry_t& g = P.geom;
     char buf[512];
@@ -1627,14 +1634,13 @@ std::string bp_tune_key(const Plan& P)
     return buf;
 }
 
-void release(Plan& P, void* p, size_t bytes)
+void plan_release(Plan& P, void* p, size_t bytes)
 {
     if (!p) return;
     cudaFree(p);
     P.allocations.erase(std::find(P.allocations.begin(), P.allocations.end(), p));
     P.device_bytes -= bytes;
 }
-}  // namespace
 
 // Times the plan's sensitivity back projection (all views, both designs set up
 // by the plan) with each design, CUDA events around the second of two runs on
@@ -1642,7 +1648,7 @@ void release(Plan& P, void* p, size_t bytes)
 // are released when the gather wins.  Synchronous (plan creation).
 recon_status_t exact_tune_bp(Plan& P)
 {
-    const std::string key = bp_tune_key(P);
+    const std::string key = geometry_key(P);
     bool known = false, gather = true;
     {
         std::lock_guard<std::mutex> lock(g_bp_tune_mutex);
@@ -1683,9 +1689,9 @@ recon_status_t exact_tune_bp(Plan& P)
     P.bp_gather = gather;
     if (gather) {
         const size_t slab = (size_t)P.eg.X * P.eg.Y * bp_slab_depth(P) * sizeof(unsigned long long);
-        release(P, P.d_bpacc, slab);
-        release(P, P.d_bpacc_t, slab);
-        release(P, P.d_bpmax, sizeof(unsigned));
+        plan_release(P, P.d_bpacc, slab);
+        plan_release(P, P.d_bpacc_t, slab);
+        plan_release(P, P.d_bpmax, sizeof(unsigned));
         P.d_bpacc = P.d_bpacc_t = nullptr;
         P.d_bpmax = nullptr;
     }

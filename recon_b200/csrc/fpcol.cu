@@ -31,13 +31,15 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <string>
 #include <type_traits>
 
 namespace rb {
 namespace exact {
 
-constexpr int kColWarps = 4;               // warps per CTA, 32 detector rows each
-constexpr int kColRows = 32 * kColWarps;   // rows per CTA
+constexpr int kColRows = 128;  // at most this many detector rows per CTA (one warp per 32; the plan picks 32, 64 or 128)
 
 // Number of b in [0, n) whose plane value fmaf(q0 + b*d, S, O) lies before t
 // (strictly when LT, else at or before); the values increase with b (d has the
@@ -332,9 +334,9 @@ __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, cons
 // g is read [view][v][u]; out is written in LAYOUT: rows [view][v][u],
 // detector columns [view][u][v] (a warp's 32 rows store 128 contiguous bytes)
 // or, with MIRROR, mirrored row pairs (a lane stores its pair at once).  A CTA
-// takes detector column u of one view and rows vstart .. vstart + kColRows - 1:
+// takes detector column u of one view and rows vstart .. vstart + blockDim.x - 1:
 // from the tile list {view, u | vstart << 16} (blockIdx.x indexes it) or,
-// without one, u = blockIdx.x, vstart = blockIdx.y * kColRows, view = view0 +
+// without one, u = blockIdx.x, vstart = blockIdx.y * blockDim.x, view = view0 +
 // blockIdx.z.
 // MIRROR: rows come in mirrored pairs (see walk_rows_mirror); the CTA's rows
 // are lower rows (below Nv/2) and each lane also produces its mirror row.
@@ -359,7 +361,7 @@ __global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const 
     } else {
         view = view0 + blockIdx.z;
         u = (int)blockIdx.x;
-        vstart = (int)blockIdx.y * kColRows;
+        vstart = (int)(blockIdx.y * blockDim.x);
     }
     const int Zp = G.Z + 2;
     const float4 T = __ldg(txy + (size_t)view * G.Nu + u);
@@ -634,14 +636,36 @@ static int column_block_side(const Plan& P)
     return (side >= E.X && side >= E.Y) ? 0 : side;
 }
 
-// The rows of view n's tiles: blocks of kColRows rows (from the first) inside
-// its rectangle of rays; mirror plans take the lower rows of the rectangle and
-// of its mirror image.
+// The rows of view n's tiles: blocks of P.col_rows rows (from the first)
+// inside its rectangle of rays; mirror plans take the lower rows of the
+// rectangle and of its mirror image.
 static void column_rows(const Plan& P, const int4& r, int* v0, int* v1)
 {
     const int Nv = P.eg.Nv;
     *v0 = P.z_mirror ? std::min(r.z, Nv - 1 - r.w) : r.z;
     *v1 = P.z_mirror ? std::min(std::max(r.w, Nv - 1 - r.z), Nv / 2 - 1) : r.w;
+}
+
+// Rows per CTA before any measurement: the fewest of 32, 64 and 128 that cover
+// the most rows a detector column walks in any view (so no warp of a CTA is
+// idle), 128 beyond.
+int exact_column_rows_default(const Plan& P, const std::vector<int4>& rect)
+{
+    int most = 0;
+    for (const int4& r : rect) {
+        if (r.y < r.x) continue;
+        int v0, v1;
+        column_rows(P, r, &v0, &v1);
+        most = std::max(most, v1 - v0 + 1);
+    }
+    return most <= 32 ? 32 : most <= 64 ? 64 : exact::kColRows;
+}
+
+static void free_tiles(Plan& P, RayTiles& T)
+{
+    if (T.d && !T.prefix.empty()) plan_release(P, T.d, (size_t)T.prefix.back() * sizeof(uint2));
+    T.d = nullptr;
+    T.prefix.clear();
 }
 
 static recon_status_t upload_tiles(Plan& P, RayTiles& T, const std::vector<uint2>& tiles)
@@ -660,8 +684,11 @@ recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect)
 {
     const unsigned nv = P.nviews;
     const ExactGeom& E = P.eg;
+    free_tiles(P, P.col_tiles);
+    for (RayTiles& T : P.col_btiles) free_tiles(P, T);
     P.col_block = column_block_side(P);
     P.col_btiles.clear();
+    const int step = P.col_rows;
     if (P.col_block == 0) {
         P.col_tiles.prefix.assign(nv + 1, 0);
         std::vector<uint2> tiles;
@@ -672,7 +699,7 @@ recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect)
             int v0, v1;
             column_rows(P, r, &v0, &v1);
             for (int u = r.x; u <= r.y; ++u)
-                for (int vs = v0; vs <= v1; vs += exact::kColRows)
+                for (int vs = v0; vs <= v1; vs += step)
                     tiles.push_back(make_uint2(n, (unsigned)u | ((unsigned)vs << 16)));
         }
         P.col_tiles.prefix[nv] = (unsigned)tiles.size();
@@ -708,7 +735,7 @@ recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect)
         for (int u = r.x; u <= r.y; ++u)
             for (unsigned long long m = mask[(size_t)n * E.Nu + u]; m; m &= m - 1) {
                 const int b = __builtin_ctzll(m);
-                for (int vs = v0; vs <= v1; vs += exact::kColRows)
+                for (int vs = v0; vs <= v1; vs += step)
                     tiles[b].push_back(make_uint2(n, (unsigned)u | ((unsigned)vs << 16)));
             }
     }
@@ -786,7 +813,7 @@ static recon_status_t launch_column_blocks(Plan& P, const float* vol, unsigned f
             if (nt == 0) continue;
             const int4 blk = make_int4(bx * side, std::min((bx + 1) * side, E.X), by * side,
                                        std::min((by + 1) * side, E.Y));
-            kernel<<<nt, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, T.d + t0, first, blk,
+            kernel<<<nt, P.col_rows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, T.d + t0, first, blk,
                                                      P.d_vol_z, nullptr, bout);
             RB_CUDA(cudaGetLastError());
         }
@@ -826,13 +853,13 @@ static recon_status_t launch_column(Plan& P, const float* vol, unsigned first, u
         tiles = P.col_tiles.d + t0;
     } else {
         const int rows = P.z_mirror ? E.Nv / 2 : E.Nv;
-        grid = dim3(E.Nu, (rows + exact::kColRows - 1) / exact::kColRows, count);
+        grid = dim3(E.Nu, (rows + P.col_rows - 1) / P.col_rows, count);
     }
     if (MODE != 3) RB_CHECK(exact_to_zfast(P, vol, s));
     const size_t smem = (size_t)(E.X + E.Y + 2) * sizeof(float2);
     auto kernel = column_kernel<MODE, LAYOUT, GT, OT>(P);
     if (smem > 48 * 1024) RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kernel<<<grid, exact::kColRows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, tiles, first,
+    kernel<<<grid, P.col_rows, smem, s>>>(E, P.d_txy, P.d_kxy, P.d_zp, P.d_wq, tiles, first,
                                                make_int4(0, E.X, 0, E.Y), P.d_vol_z, g, out);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
@@ -858,6 +885,70 @@ recon_status_t exact_fp_column_count(Plan& P, unsigned long long* total)
 recon_status_t exact_fp_column(Plan& P, const float* vol, unsigned first, unsigned count, float* out, cudaStream_t s)
 {
     return launch_column<0, kLayoutRows, float, float>(P, vol, first, count, nullptr, out, s);
+}
+
+// RECON_SIDDON_BP_TUNED also measures the column forward projector's rows per
+// CTA: each of 32, 64 and 128 (a warp per 32 rows; fewer rows leave no warp
+// idle where a detector column has few rows to walk, more build the column's
+// path once for more rows) is timed on a projection of up to 64 of the plan's
+// views, CUDA events around the second of two runs on the legacy stream, and
+// the fastest kept.  The choice is kept for the process per geometry and
+// device, as the back projector's.  Synchronous (plan creation).
+namespace {
+std::mutex g_fp_tune_mutex;
+std::map<std::string, int> g_fp_tune_rows;
+}  // namespace
+
+recon_status_t exact_tune_fp(Plan& P)
+{
+    if (!P.fp_column || P.nviews == 0 || P.view_rect_host.size() != P.nviews) return RECON_OK;
+    const std::string key = geometry_key(P);
+    int rows = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_fp_tune_mutex);
+        auto it = g_fp_tune_rows.find(key);
+        if (it != g_fp_tune_rows.end()) rows = it->second;
+    }
+    if (rows == 0) {
+        const unsigned nv = std::min(P.nviews, 64u);
+        float *vol = nullptr, *out = nullptr;
+        cudaError_t e = cudaMalloc(&vol, P.nvox * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&out, (size_t)nv * P.npix * sizeof(float));
+        if (e == cudaSuccess) e = cudaMemset(vol, 0, P.nvox * sizeof(float));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (e == cudaSuccess) e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        recon_status_t st = RECON_OK;
+        float best = 0.0f;
+        for (int r = 32; r <= exact::kColRows && e == cudaSuccess && st == RECON_OK; r *= 2) {
+            P.col_rows = r;
+            st = build_column_tiles(P, P.view_rect_host);
+            if (st == RECON_OK) st = exact_fp_column(P, vol, 0, nv, out, 0);
+            if (st == RECON_OK) e = cudaEventRecord(e0, 0);
+            if (e == cudaSuccess && st == RECON_OK) st = exact_fp_column(P, vol, 0, nv, out, 0);
+            if (e == cudaSuccess && st == RECON_OK) e = cudaEventRecord(e1, 0);
+            if (e == cudaSuccess && st == RECON_OK) e = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            if (e == cudaSuccess && st == RECON_OK) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && st == RECON_OK && (rows == 0 || ms < best)) {
+                best = ms;
+                rows = r;
+            }
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        cudaFree(vol);
+        cudaFree(out);
+        if (st != RECON_OK) return st;
+        if (e != cudaSuccess) return cuda_fail(e, "forward projector tuning");
+        std::lock_guard<std::mutex> lock(g_fp_tune_mutex);
+        g_fp_tune_rows.emplace(key, rows);
+    }
+    if (P.col_rows != rows) {
+        P.col_rows = rows;
+        RB_CHECK(build_column_tiles(P, P.view_rect_host));
+    }
+    return RECON_OK;
 }
 
 // The MLEM ratio (MODE 1: times w, Siddon back projectors; MODE 2: without w,

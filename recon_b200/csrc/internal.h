@@ -138,6 +138,7 @@ struct Plan {
     // column forward projector over xy blocks (volumes larger than L2): block
     // side in voxels (0: one pass over the whole volume), the blocks' tiles,
     // and block sums [nviews][u][v] where the output cannot hold them
+    int col_rows = 128;            // detector rows per CTA of the column forward projector (32, 64, 128)
     bool col_pairs = false;        // the gather's inputs in mirrored row pairs (kLayoutPairs)
     float* d_wq_pairs = nullptr;   // d_wq in mirrored row pairs (the sensitivity's input)
     int col_block = 0;
@@ -145,6 +146,7 @@ struct Plan {
     std::vector<RayTiles> col_btiles;
     float* d_col_acc = nullptr;
     int4* d_view_rect = nullptr;  // [view] {u_min, u_max, v_min, v_max} of the rays crossing the volume
+    std::vector<int4> view_rect_host;  // the same on the host
     int sino_v0 = 0, sino_v1 = -1;  // rows some ray crossing the volume reaches, over all views
     bool sino_rows_known = false;   // EXACT culling ran: sino_v0..sino_v1 bound every row the plan reads
     std::vector<RayTiles> bp_tiles;
@@ -255,6 +257,10 @@ recon_status_t exact_tune_bp(Plan& P);
 // forward projection by detector columns (fpcol.cu)
 bool exact_fp_column_suits(const Plan& P);
 bool exact_pairs_suit(const Plan& P);
+recon_status_t exact_tune_fp(Plan& P);
+int exact_column_rows_default(const Plan& P, const std::vector<int4>& rect);
+std::string geometry_key(const Plan& P);
+void plan_release(Plan& P, void* p, size_t bytes);
 recon_status_t build_wq_pairs(Plan& P);
 recon_status_t build_column_tiles(Plan& P, const std::vector<int4>& rect);
 recon_status_t exact_fp_column(Plan& P, const float* vol, unsigned first, unsigned count, float* out, cudaStream_t s);

@@ -42,8 +42,8 @@ def test_exports_every_declared_function():
 def test_default_options():
     o = L.Options()
     assert L.lib().recon_default_options(C.byref(o)) == 0
-    assert (o.arith, o.sum, o.sino, o.bp, o.voxel_mode, o.device, o.siddon_bp, o.fp_block) == (
-        L.ARITH_EXACT, L.SUM_KAHAN, L.SINO_F32, L.BP_SIDDON, L.VOXEL_GEOMETRIC, 0, L.SIDDON_BP_AUTO, 0)
+    assert (o.arith, o.sum, o.sino, o.bp, o.voxel_mode, o.device, o.siddon_bp, o.fp_block, o.fp_rows) == (
+        L.ARITH_EXACT, L.SUM_KAHAN, L.SINO_F32, L.BP_SIDDON, L.VOXEL_GEOMETRIC, 0, L.SIDDON_BP_AUTO, 0, 0)
 
 
 def _cfg_text(extra=""):
@@ -147,6 +147,11 @@ def test_plan_rejects_bad_geometry():
         o.fp_block = bad_block
         assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1, bad_block
         assert "fp_block" in lib.recon_last_error().decode()
+    o.fp_block = 0
+    for bad_rows in (-32, 16, 96, 256):
+        o.fp_rows = bad_rows
+        assert lib.recon_plan_create(C.byref(geometry(small_cfg())), C.byref(o), C.byref(h)) == 1, bad_rows
+        assert "fp_rows" in lib.recon_last_error().decode()
 
 
 @pytest.mark.skipif(have_gpu(), reason="checks the no-device path")
