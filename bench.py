@@ -512,6 +512,33 @@ def reference_gpu_leg(O, geo, cfg, vol, gviews: dict) -> dict | None:
                       f"extrapolated x{n}"}
 
 
+def small_full_iteration(R, O, threads: int, prefix: int) -> dict:
+    """The extrapolation above, checked where it can be measured in full: one
+    MLEM iteration of the 64^3 / 90-view / 128^2 workload (configs.CPU_SMALL)
+    with the reference's step-synchronous kernels built for the host, every
+    view run to its last step, against the same views predicted from their
+    first `prefix` step launches."""
+    import numpy as np
+
+    from recon_b200.configs import CPU_SMALL, geom_dict
+
+    cfg = dict(CPU_SMALL)
+    geo = O.Geom.from_dict(geom_dict(cfg))
+    n = int(cfg["NumProj"])
+    rng = np.random.default_rng(1)
+    f = np.ones(geo.nvox, np.float32)
+    ht = np.zeros(geo.nvox, np.float32)
+    full = predicted = 0.0
+    for v in range(n):
+        gview = rng.random(geo.npix).astype(np.float32)
+        predicted += ref_view_seconds(R, O, geo, cfg, v, prefix, f, gview, ht)[0]
+        full += ref_view_seconds(R, O, geo, cfg, v, 1 << 30, f, gview, ht)[1]
+    return {"workload": "cpu_small_64cube_90x128x128", "threads": threads, "measured_s_per_iteration": full,
+            "predicted_s_per_iteration": predicted, "predicted_over_measured": predicted / full,
+            "sample": f"every view of one MLEM iteration run to its last step, and predicted from its first "
+                      f"{prefix} step launches"}
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -580,6 +607,7 @@ def run_reference(args):
         rg = {"error": str(e)}
     if rg is not None:
         out["reference_gpu"] = rg
+    out["extrapolation_check"] = small_full_iteration(R, O, threads, prefix)
     print(json.dumps(out))
 
 
