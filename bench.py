@@ -571,8 +571,9 @@ def run_reference(args):
     # the GPU arm's inputs for these views: the same phantom, projected (here in
     # FP64, there by the FP32 EXACT projector: equal to ~1e-7 relative) and the
     # same Poisson draws (noisy_views: view n from seed * 100000 + n)
+    gpu_views = [k * n // 8 for k in range(8)]  # the reference's CUDA build: 8 evenly spaced views
     gviews = {}
-    for v in sorted(set(views)):
+    for v in sorted(set(views) | set(gpu_views)):
         img = np.zeros(geo.npix)
         O.lib().orc_x_fp_view(geo, float(np.float32(v) * dang), vol, img)
         gviews[v] = noisy(img, cfg["I0"], cfg["seed"] * 100000 + v).astype(np.float32)
@@ -602,7 +603,7 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     try:
-        rg = reference_gpu_leg(O, geo, cfg, vol, {v: gviews[v] for v in sorted(set(views))[:4]})
+        rg = reference_gpu_leg(O, geo, cfg, vol, {v: gviews[v] for v in gpu_views})
     except Exception as e:  # pragma: no cover
         rg = {"error": str(e)}
     if rg is not None:
@@ -835,9 +836,23 @@ def main():
                            "traffic_source": TRAFFIC_PROFILE if dom[3] is not None else None,
                            "algorithmic_bytes_per_launch": dom[2], "launch_ms": dom[1]}
         b_iter = 8.0 * isects + 4.0 * npix * nviews + 12.0 * nvox
+        b_comp = 4.0 * npix * nviews + 12.0 * nvox  # the bytes no design avoids: g once, f and sens read, f written
         out["iteration_roofline"] = {"bytes_per_iteration": b_iter, "achieved_gbs": b_iter / (ms_step * 1e-3) / 1e9,
                                      "frac": b_iter / (ms_step * 1e-3) / 1e9 / hbm,
+                                     "compulsory_bytes": b_comp,
+                                     "compulsory_frac": b_comp / (ms_step * 1e-3) / 1e9 / hbm,
                                      "fp_ms": t_fp, "bp_ms": t_bp}
+        # the sensitivity image: one back projection of w, computed once per plan (outside the iterations)
+        sens = P.new_volume(0.0)
+        P.sensitivity(sens)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record()
+        P.sensitivity(sens)
+        s1.record()
+        torch.cuda.synchronize()
+        out["sensitivity_ms"] = s0.elapsed_time(s1)
+        del sens
     out["e2e"] = e2e
     out["clocks"] = clk
     if world == 1:
