@@ -211,6 +211,15 @@ recon_status_t recon_plan_forward_projector(recon_plan_t plan, int* design);
  * (no vertical detector offset Dz).  Results are the same either way.  No
  * counterpart in the reference. */
 recon_status_t recon_plan_mirror_pairs(recon_plan_t plan, int* paired);
+/* *quarter = 1 when an EXACT plan's views come in quarter turns about a
+ * square volume (Xdim = Ydim, even, XVoxSize = YVoxSize, NumProj a multiple
+ * of 4 with view n + NumProj/4 at exactly angle(n) + 90 degrees).  The plan
+ * then derives the ray tables of views NumProj/4 .. NumProj-1 from the first
+ * quarter's by exact quarter turns, so both projectors give column (x, y) at
+ * view n + NumProj/4 exactly the lengths of column (Xdim-1-y, x) at view n,
+ * and the mirror-paired gather back projector finds each set of lengths once
+ * for four columns.  No counterpart in the reference. */
+recon_status_t recon_plan_quarter_turns(recon_plan_t plan, int* quarter);
 /* *rows = the detector rows per CTA of the plan's detector-column forward
  * projector (32, 64 or 128: the fewest that cover a column's rows, or the
  * fastest measured with RECON_SIDDON_BP_TUNED), 0 for other forward
@@ -234,8 +243,8 @@ recon_status_t recon_fp_views(recon_plan_t plan, const float* d_vol, unsigned in
  * (hf_siddon_class.hpp:313-352). */
 recon_status_t recon_bp_view(recon_plan_t plan, const float* d_img, float angle_deg, float* d_vol,
                              void* stream);
-/* Sum over views first..first+count-1 of the back projections of d_sino;
- * d_vol is overwritten. */
+/* Sum over views first..first+count-1 of the back projections of d_sino,
+ * which holds those count views back to back; d_vol is overwritten. */
 recon_status_t recon_bp_views(recon_plan_t plan, const float* d_sino, unsigned int first,
                               unsigned int count, float* d_vol, void* stream);
 /* Sensitivity image: back projection of an all-ones sinogram over all views.

@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
         "recon_plan_siddon_bp": (st, [P, ip]),
         "recon_plan_forward_projector": (st, [P, C.POINTER(C.c_int)]),
         "recon_plan_mirror_pairs": (st, [P, C.POINTER(C.c_int)]),
+        "recon_plan_quarter_turns": (st, [P, C.POINTER(C.c_int)]),
         "recon_plan_column_rows": (st, [P, C.POINTER(C.c_int)]),
         "recon_march_fp_view": (st, [P, P, f, C.c_int, P, P]),
         "recon_fp_view": (st, [P, P, f, P, P]),
@@ -153,7 +154,7 @@ def exported_symbols() -> list[str]:
     """Names of the C ABI functions this binding expects (all of include/recon_b200.h)."""
     return [
         "recon_abi_version", "recon_last_error", "recon_default_options", "recon_geometry_from_cfg",
-        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_plan_mirror_pairs", "recon_plan_column_rows", "recon_fp_view", "recon_fp_views",
+        "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_plan_mirror_pairs", "recon_plan_quarter_turns", "recon_plan_column_rows", "recon_fp_view", "recon_fp_views",
         "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_march_fp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
         "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_count_projector_pairs", "recon_set_ones", "recon_divide1", "recon_multiply1",

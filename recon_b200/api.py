@@ -151,6 +151,13 @@ class Plan:
         return bool(d.value)
 
     @property
+    def quarter_turns(self) -> bool:
+        """True when an EXACT plan's views come in exact quarter turns about a square volume."""
+        d = C.c_int(0)
+        check(lib().recon_plan_quarter_turns(self._h, C.byref(d)))
+        return bool(d.value)
+
+    @property
     def forward_projector(self) -> int:
         """The forward projector of an EXACT plan: FP_COLUMNS or FP_RAY_WALK."""
         d = C.c_int(-1)

@@ -372,6 +372,13 @@ recon_status_t recon_plan_mirror_pairs(recon_plan_t plan, int* paired)
     return RECON_OK;
 }
 
+recon_status_t recon_plan_quarter_turns(recon_plan_t plan, int* quarter)
+{
+    if (!plan || !quarter) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    *quarter = (plan->opt.arith == RECON_ARITH_EXACT && plan->quarter) ? 1 : 0;
+    return RECON_OK;
+}
+
 recon_status_t recon_plan_siddon_bp(recon_plan_t plan, int* design)
 {
     if (!plan || !design) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");

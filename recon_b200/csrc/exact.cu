@@ -98,6 +98,35 @@ __global__ void xy_table_kernel(GeomD G, const float* __restrict__ angles, unsig
     if (u == 0) cs[view] = make_float2((float)c, (float)s);
 }
 
+// Views a quarter turn apart.  With a square volume (X = Y, equal x and y voxel
+// sizes, P0 = -X vox / 2 on both axes) and view n + q at angle(n) + 90 degrees,
+// ray (view n + q, u) is ray (view n, u) turned about the z axis, (x, y) ->
+// (y, -x) by xy_table_kernel's formulas: its x planes are view n's y planes
+// and its y plane k is view n's x plane X - k.  So its entries are
+//     {Sx, Ox, Sy, Oy}' = {Sy, Oy, -Sx, Ox},  {kcx, kcy}' = {kcy, X - kcx},
+// as fmaf(k - (X - kc), -S, O) = fmaf((X - k) - kc, S, O) bit for bit.  Views
+// q .. 4q-1 are derived this way from views 0 .. q-1 (one thread per (view n <
+// q, u)), which makes every length either projector gives to (column (i, j),
+// view n + q) the one it gives to (column (X-1-j, i), view n), bit for bit.
+__global__ void quarter_turn_table_kernel(int X, int Nu, unsigned q, float4* __restrict__ txy, int2* __restrict__ kxy,
+                                          float2* __restrict__ cs)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned n = blockIdx.y;
+    if (u >= Nu) return;
+    float4 T = txy[(size_t)n * Nu + u];
+    int2 K = kxy[(size_t)n * Nu + u];
+    float2 c = cs[n];
+    for (unsigned r = 1; r < 4; ++r) {
+        T = make_float4(T.z, T.w, -T.x, T.y);
+        K = make_int2(K.y, X - K.x);
+        c = make_float2(-c.y, c.x);  // {cos, sin} of the angle plus 90 degrees
+        txy[(size_t)(n + r * q) * Nu + u] = T;
+        kxy[(size_t)(n + r * q) * Nu + u] = K;
+        if (u == 0) cs[n + r * q] = c;
+    }
+}
+
 __global__ void z_table_kernel(GeomD G, ZParam* __restrict__ zp)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -924,6 +953,239 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_pairs_kernel(
 }
 
 
+// The pair gather over all of a plan's views where views a quarter turn apart
+// are exact rotations of each other (Plan::quarter, tables from
+// quarter_turn_table_kernel: N = 4Q views, column c at view n + Q is column
+// rho(c) = (X-1-j, i) at view n, bit for bit).  The candidate rows and lengths
+// found for base column c0 = (i, j) at view m therefore serve the four columns
+// of its orbit
+//     d_0 = (i, j),  d_1 = (j, X-1-i),  d_2 = (X-1-i, X-1-j),  d_3 = (X-1-j, i)
+// (d_r = rho^-r(c0)) at views m, m + Q, m + 2Q, m + 3Q (mod N): a lane finds a
+// voxel pair's rows and lengths once and loads four value pairs for them, one
+// per view.  Base columns tile the quadrant i, j < X/2 (one orbit each); a
+// CTA's 4 x 2 base columns are 8 warps as in bp_gather_pairs_kernel.  Column
+// d_r sums its views in the order rQ .. N-1, 0 .. rQ-1, each piece's further
+// candidate rows after its first ones, into the same registers: deterministic,
+// the same lengths as bp_gather_pairs_kernel, the sums in another order.
+// Dynamic shared memory: the rows' z planes (Nv float4), then the epilogue's
+// staging area [warp][d_r][lower voxels, mirrors][PS * 32].
+template <int EPI, class ST, int PS>
+__global__ void __launch_bounds__(kGatherWarps * 32, 2) bp_gather_quarter_kernel(
+    ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
+    const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned nview, const ST* __restrict__ vals,
+    size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens, unsigned long long* __restrict__ npairs)
+{
+    extern __shared__ float4 szq[];
+    __shared__ GatherView sview[kGatherWarps][32];
+    constexpr int NE = 8 * PS * 32;  // staged entries per warp
+    float* const stage = reinterpret_cast<float*>(szq + G.Nv);
+    for (int q = threadIdx.x; q < G.Nv; q += blockDim.x) {
+        const ZParam z = zp[q];
+        const float kc = (float)z.kc;
+        szq[q] = (z.S > 0.0f) ? make_float4(z.S, z.O, kc, kc - 1.0f) : make_float4(z.S, z.O, kc - 1.0f, kc);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int H = G.X / 2;
+    const int i0 = blockIdx.x * kGatherTileX, j0 = blockIdx.y * (kGatherWarps / kGatherTileX);
+    const int i = i0 + warp % kGatherTileX, j = j0 + warp / kGatherTileX;
+    const bool active = i < H && j < H;
+    const unsigned nview_w = active ? nview : 0u;
+    const unsigned Q = nview / 4u;
+    GatherView* sv = sview[warp];
+    const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
+    const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
+    const float oz_lo = C.oz - 0.002f, oz_hi = C.oz + 0.002f;  // margins as in bp_gather_kernel
+    const float dz32 = 32.0f * G.vox[2];
+    const int Zh = G.Z / 2;
+    const unsigned top = (unsigned)G.Nv - 1u;
+    const unsigned Nh = (unsigned)G.Nv / 2u, Np = Nh + 1u;  // pairs per detector column
+    for (int k0 = 0; k0 < Zh; k0 += 32 * PS) {
+        const float fk0 = (float)(k0 + lane);
+        const float zl0 = fmaf(fk0, G.vox[2], G.P0[2]), zh0 = zl0 + G.vox[2];
+        const int nslot = min(PS, max(0, (Zh - k0 - lane + 31) / 32));
+        float acc[4][PS], accm[4][PS];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int s = 0; s < PS; ++s) {
+                acc[r][s] = 0.0f;
+                accm[r][s] = 0.0f;
+            }
+        // one pair of rows {a, Nv-1-a} (a <= Nv/2) of the four views, length L
+        auto add4 = [&](int s, float L, const ST* const* cols, unsigned a) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const auto p = load_pair_raw(cols[r] + 2u * a);
+                acc[r][s] = (EPI == 2) ? acc[r][s] + 1.0f : fmaf(L, widen_lo(p), acc[r][s]);
+                accm[r][s] = (EPI == 2) ? accm[r][s] + 1.0f : fmaf(L, widen_hi(p), accm[r][s]);
+            }
+        };
+        // detector column u of view m: its piece [A, B], row coefficients and
+        // steps; cols[r] = view m + rQ's values from pair 0 of column u
+        auto piece = [&](float A, float B, float ca, float cb, float pa, float pb, bool single, bool behind,
+                         const ST* const* cols) {
+            auto length = [&](int s, int v) {  // row v's length through lower voxel s of this lane
+                const float4 zr = szq[v];
+                const float t = fk0 + (float)(32 * s);
+                const float lo = fmaf(t - zr.z, zr.x, zr.y), hi = fmaf(t - zr.w, zr.x, zr.y);
+                return fminf(B, hi) - fmaxf(A, lo);
+            };
+            if (behind) {  // a piece behind the source: every row is a candidate
+#pragma unroll
+                for (int s = 0; s < PS; ++s)
+                    if (s < nslot)
+                        for (int v = 0; v < G.Nv; ++v) {
+                            const float L = length(s, v);
+                            if (!(L > 0.0f)) continue;
+                            // row v and its mirror from pair min(v, Nv-1-v), in order
+                            const bool lower = (unsigned)v < Nh;
+                            const unsigned a = lower ? (unsigned)v : top - v;
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                const auto p = load_pair_raw(cols[r] + 2u * a);
+                                const float xv = lower ? widen_lo(p) : widen_hi(p);
+                                const float xm = lower ? widen_hi(p) : widen_lo(p);
+                                acc[r][s] = (EPI == 2) ? acc[r][s] + 1.0f : fmaf(L, xv, acc[r][s]);
+                                accm[r][s] = (EPI == 2) ? accm[r][s] + 1.0f : fmaf(L, xm, accm[r][s]);
+                            }
+                        }
+                return;
+            }
+            // first candidate row of every lower voxel, clamped to row Nv/2 as in
+            // bp_gather_pairs_kernel: lengths found once, then four loads each
+            const float P0a = fmaf(zl0, ca, oz_lo);
+            const float P1b = single ? 0.0f : fmaf(zh0, cb, oz_hi);
+            unsigned av[PS], more = 0u;
+            float L[PS];
+#pragma unroll
+            for (int s = 0; s < PS; ++s) {
+                const float f0 = fmaf((float)s, pa, P0a);
+                av[s] = min(__float2uint_ru(f0), Nh);
+                L[s] = length(s, (int)av[s]);
+                if (!single) {
+                    const float f1 = fmaf((float)s, pb, P1b);
+                    if ((float)(av[s] + 1u) <= f1) more |= 1u << s;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                decltype(load_pair_raw(cols[0])) x[PS];
+#pragma unroll
+                for (int s = 0; s < PS; ++s) x[s] = load_pair_raw(cols[r] + 2u * av[s]);
+#pragma unroll
+                for (int s = 0; s < PS; ++s)
+                    if (L[s] > 0.0f) {
+                        acc[r][s] = (EPI == 2) ? acc[r][s] + 1.0f : fmaf(L[s], widen_lo(x[s]), acc[r][s]);
+                        accm[r][s] = (EPI == 2) ? accm[r][s] + 1.0f : fmaf(L[s], widen_hi(x[s]), accm[r][s]);
+                    }
+            }
+            // further candidates (rare), over the bounds of both piece ends
+            if (__any_sync(0xffffffffu, more != 0u)) {
+                const float P0b = fmaf(zl0, cb, oz_lo), P1a = fmaf(zh0, ca, oz_hi);
+#pragma unroll
+                for (int s = 0; s < PS; ++s) {
+                    if (!((more >> s) & 1u)) continue;
+                    const float f0 = fminf(fmaf((float)s, pa, P0a), fmaf((float)s, pb, P0b));
+                    const float f1 = fmaxf(fmaf((float)s, pa, P1a), fmaf((float)s, pb, P1b));
+                    const int a = max(0, __float2int_ru(f0));
+                    const int b = min((int)Nh, __float2int_rd(f1));
+                    for (int v = a + 1; v <= b; ++v) {
+                        const float Lv = length(s, v);
+                        if (Lv > 0.0f) add4(s, Lv, cols, (unsigned)v);
+                    }
+                }
+            }
+        };
+        for (unsigned vb = 0; vb < nview_w; vb += 32) {
+            const unsigned nb = min(32u, nview_w - vb);
+            if ((unsigned)lane < nb)  // lane q sets up view vb + q
+                sv[lane] = gather_view(G, C, txy, kxy, cs, vb + lane, i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo, dz32);
+            __syncwarp();
+            for (unsigned q = 0; q < nb; ++q) {
+                const unsigned m = vb + q;
+                const ST* vm[4];  // views m + rQ (mod N) from detector column 0
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    unsigned w = m + (unsigned)r * Q;
+                    if (w >= nview) w -= nview;
+                    vm[r] = vals + (size_t)w * view_stride;
+                }
+                auto column = [&](int u, const ST** cols) {
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) cols[r] = vm[r] + (size_t)u * Np * 2;
+                };
+                const int ulo = sv[q].u_lo, uhi = sv[q].u_hi;
+                const unsigned fl = sv[q].flags;
+#pragma unroll 1
+                for (int sl = 0; sl < 2; ++sl) {
+                    if (ulo + sl > uhi) break;
+                    if (!((fl >> sl) & 1u)) continue;  // the rays miss the column
+                    const float4 ab = sv[q].ab[sl];
+                    const float2 cc = sv[q].c[sl];
+                    const ST* cols[4];
+                    column(ulo + sl, cols);
+                    piece(ab.x, ab.y, cc.x, cc.y, ab.z, ab.w, (fl >> (2 + sl)) & 1u, (fl >> (4 + sl)) & 1u, cols);
+                }
+                // a column wider than two detector pitches: set up here
+                for (int u = ulo + 2; u <= uhi; ++u) {
+                    const float4 T = __ldg(txy + (size_t)m * G.Nu + u);
+                    const int2 K = __ldg(kxy + (size_t)m * G.Nu + u);
+                    const float xa = plane_t(i, T.x, T.y, K.x), xb = plane_t(i + 1, T.x, T.y, K.x);
+                    const float ya = plane_t(j, T.z, T.w, K.y), yb = plane_t(j + 1, T.z, T.w, K.y);
+                    const float A = fmaxf(fminf(xa, xb), fminf(ya, yb));
+                    const float B = fminf(fmaxf(xa, xb), fmaxf(ya, yb));
+                    if (!(A < B)) continue;
+                    const float ca = C.ez / (A + G.Rf), cb = C.ez / (B + G.Rf);
+                    const ST* cols[4];
+                    column(u, cols);
+                    piece(A, B, ca, cb, dz32 * ca, dz32 * cb, false, !(A + G.Rf > 1e-3f * G.Rf), cols);
+                }
+            }
+            __syncwarp();  // the next batch rewrites sv
+        }
+        if (EPI == 2) {  // pair counts of the four columns
+            unsigned long long c = 0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int s = 0; s < PS; ++s)
+                    if (s < nslot) c += (unsigned long long)acc[r][s] + (unsigned long long)accm[r][s];
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0 && c) atomicAdd(npairs, c);
+            continue;
+        }
+        // entry ((r * 2 + h) * PS + s) * 32 + lane: column d_r, lower voxel (h = 0)
+        // k0 + lane + 32 s or its mirror (h = 1)
+        float* const st = stage + warp * NE;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int s = 0; s < PS; ++s) {
+                st[((r * 2) * PS + s) * 32 + lane] = acc[r][s];
+                st[((r * 2 + 1) * PS + s) * 32 + lane] = accm[r][s];
+            }
+        __syncthreads();
+        // the CTA's epilogue, one voxel per thread, warps fastest (a column
+        // tile's x neighbours adjacent)
+        const size_t plane = (size_t)G.X * G.Y;
+        for (int q = threadIdx.x; q < kGatherWarps * NE; q += blockDim.x) {
+            const int w = q % kGatherWarps, e = q / kGatherWarps;
+            const int bi = i0 + w % kGatherTileX, bj = j0 + w / kGatherTileX;
+            if (bi >= H || bj >= H) continue;
+            const int r = e / (2 * PS * 32), h = (e / (PS * 32)) & 1, k = k0 + e % (PS * 32);
+            if (k >= Zh) continue;
+            const int x = (r == 0) ? bi : (r == 1) ? bj : (r == 2) ? G.X - 1 - bi : G.X - 1 - bj;
+            const int y = (r == 0) ? bj : (r == 1) ? G.X - 1 - bi : (r == 2) ? G.X - 1 - bj : bi;
+            const int z = h ? G.Z - 1 - k : k;
+            const size_t v = (size_t)z * plane + (size_t)y * G.X + (size_t)x;
+            const float hv = stage[w * NE + e];
+            vol[v] = (EPI == 1) ? gather_update(vol[v], hv, sens[v]) : hv;
+        }
+        __syncthreads();  // the next chunk rewrites the staging area
+    }
+}
+
 // A sinogram [view][v][u] times w into mirrored row pairs (kLayoutPairs), 32 (u)
 // x 32 (pair) tiles: both rows of each pair read along u through shared memory,
 // w (detector columns, wq) and the pairs along the pair index.
@@ -1135,13 +1397,34 @@ static exact::GeomD geom_d(const Plan& P)
     return G;
 }
 
+// The plan's views come in quarter turns of a square volume (see
+// quarter_turn_table_kernel): N = 4q views, view n + q at exactly angle(n) + 90
+// degrees.
+static bool quarter_turn_suits(const Plan& P)
+{
+    const recon_geometry_t& g = P.geom;
+    if (P.nviews < 4 || P.nviews % 4 != 0) return false;
+    if (g.vox.Xdim != g.vox.Ydim || g.vox.Xdim % 2 != 0 || g.vox.XVoxSize != g.vox.YVoxSize) return false;
+    const unsigned q = P.nviews / 4;
+    for (unsigned n = 0; n < 3 * q; ++n)
+        if ((double)P.view_angles[n + q] != (double)P.view_angles[n] + 90.0) return false;
+    return true;
+}
+
 recon_status_t build_exact_tables(Plan& P, cudaStream_t s)
 {
     exact::GeomD G = geom_d(P);
+    P.quarter = quarter_turn_suits(P);
     if (P.nviews) {
-        exact::xy_table_kernel<<<dim3((G.Nu + 127) / 128, P.nviews), 128, 0, s>>>(G, P.d_angles, 0u, P.nviews,
-                                                                                 P.d_txy, P.d_kxy, P.d_cs);
+        const unsigned direct = P.quarter ? P.nviews / 4 : P.nviews;  // views computed from their angles
+        exact::xy_table_kernel<<<dim3((G.Nu + 127) / 128, direct), 128, 0, s>>>(G, P.d_angles, 0u, direct, P.d_txy,
+                                                                              P.d_kxy, P.d_cs);
         RB_CUDA(cudaGetLastError());
+        if (P.quarter) {
+            exact::quarter_turn_table_kernel<<<dim3((G.Nu + 127) / 128, direct), 128, 0, s>>>(
+                G.dims[0], G.Nu, direct, P.d_txy, P.d_kxy, P.d_cs);
+            RB_CUDA(cudaGetLastError());
+        }
     }
     exact::z_table_kernel<<<(G.Nv + 127) / 128, 128, 0, s>>>(G, P.d_zp);
     RB_CUDA(cudaGetLastError());
@@ -1703,12 +1986,7 @@ recon_status_t exact_tune_bp(Plan& P)
 // arrays, within the 227 KB a block may use.
 int exact_bp_gather_max_rows() { return 12288; }
 
-// SLOTS: voxels per lane for bp_gather_kernel, voxel pairs per lane for the
-// mirror kernel (MIRROR).
-template <int EPI, class ST, int SLOTS, bool MIRROR = false>
-static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_stride, unsigned first,
-                                          unsigned count, float* vol, const float* sens, cudaStream_t s,
-                                          unsigned long long* npairs = nullptr)
+static exact::GatherConst gather_const(const Plan& P, const float* vol, const float* sens)
 {
     const ExactGeom& E = P.eg;
     exact::GatherConst C;
@@ -1718,6 +1996,59 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
     C.oz = (float)(-((double)E.Dz + E.vd0) / E.dv);
     C.vec4 = (E.X % 4 == 0) && (reinterpret_cast<uintptr_t>(vol) % 16 == 0) &&
              (reinterpret_cast<uintptr_t>(sens) % 16 == 0);
+    return C;
+}
+
+// bp_gather_quarter_kernel's shared memory: the rows' z planes and its staging
+// area (dynamic), the per-warp view set-up (static).
+template <int PS>
+static size_t quarter_dynamic_smem(const Plan& P)
+{
+    return (size_t)P.eg.Nv * sizeof(float4) + sizeof(float) * exact::kGatherWarps * 8 * PS * 32;
+}
+constexpr size_t kQuarterStaticSmem = sizeof(exact::GatherView) * 32 * exact::kGatherWarps;
+
+// The quarter-turn gather serves this call: all of the plan's views, which
+// come in exact quarter turns, in mirrored row pairs, within a block's shared
+// memory.
+template <int PS>
+static bool quarter_gather_serves(const Plan& P, unsigned first, unsigned count)
+{
+    return P.quarter && P.col_pairs && P.z_mirror && first == 0 && count == P.nviews && count >= 4 &&
+           quarter_dynamic_smem<PS>(P) + kQuarterStaticSmem <= 227 * 1024;
+}
+
+template <int EPI, class ST, int PS>
+static recon_status_t launch_gather_quarter(Plan& P, const ST* vals, size_t view_stride, float* vol,
+                                            const float* sens, cudaStream_t s, unsigned long long* npairs)
+{
+    const ExactGeom& E = P.eg;
+    const exact::GatherConst C = gather_const(P, vol, sens);
+    const size_t smem = quarter_dynamic_smem<PS>(P);
+    auto kernel = exact::bp_gather_quarter_kernel<EPI, ST, PS>;
+    if (smem + kQuarterStaticSmem > 48 * 1024)
+        RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
+    const int H = E.X / 2;  // base columns: the quadrant x, y < X/2
+    const dim3 grid((H + tx - 1) / tx, (H + ty - 1) / ty);
+    kernel<<<grid, exact::kGatherWarps * 32, smem, s>>>(E, C, P.d_txy, P.d_kxy, P.d_cs, P.d_zp, P.nviews, vals,
+                                                         view_stride, vol, sens, npairs);
+    RB_CUDA(cudaGetLastError());
+    return RECON_OK;
+}
+
+// SLOTS: voxels per lane for bp_gather_kernel, voxel pairs per lane for the
+// mirror kernels (MIRROR).
+template <int EPI, class ST, int SLOTS, bool MIRROR = false>
+static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_stride, unsigned first,
+                                          unsigned count, float* vol, const float* sens, cudaStream_t s,
+                                          unsigned long long* npairs = nullptr)
+{
+    const ExactGeom& E = P.eg;
+    if constexpr (MIRROR)
+        if (quarter_gather_serves<SLOTS>(P, first, count))
+            return launch_gather_quarter<EPI, ST, SLOTS>(P, vals, view_stride, vol, sens, s, npairs);
+    const exact::GatherConst C = gather_const(P, vol, sens);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
     auto kernel = [&P] {
         if constexpr (MIRROR)
@@ -1793,7 +2124,8 @@ recon_status_t exact_bp_gather_count(Plan& P, unsigned long long* total)
     cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
     recon_status_t st = RECON_OK;
     if (e == cudaSuccess && P.nviews)
-        st = launch_gather<2, float>(P, P.d_wq, 0, 0u, P.nviews, nullptr, nullptr, 0, d);
+        st = launch_gather<2, float>(P, P.col_pairs ? P.d_wq_pairs : P.d_wq, 0, 0u, P.nviews, nullptr, nullptr, 0,
+                                     d);  // the weights in the layout the kernel reads
     if (e == cudaSuccess && st == RECON_OK) e = cudaMemcpy(total, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (st != RECON_OK) return st;

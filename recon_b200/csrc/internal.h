@@ -122,6 +122,8 @@ struct Plan {
     unsigned colsino_views = 0;   // views d_colsino holds
     bool bp_gather = false;    // Siddon back projection by the column gather (else ray-driven slabs)
     bool z_mirror = false;     // z table mirror-symmetric about z = 0: both projectors pair mirrored rows/voxels
+    bool quarter = false;      // views n + N/4 a quarter turn from view n about a square volume, their xy
+                               // tables exact rotations of view n's (the gather serves four columns a warp)
     float* d_vol_t = nullptr;  // xy-transposed copy of the projected volume [z][x][y] (ray-walk forward projector)
     bool fp_column = false;    // forward projection by detector columns (fpcol.cu), else the ray walk
     float* d_vol_z = nullptr;  // z-fastest copy of the projected volume with a zero layer at each end:

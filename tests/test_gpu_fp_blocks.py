@@ -23,8 +23,8 @@ if not torch.cuda.is_available():
     pytest.skip("no CUDA device", allow_module_level=True)
 
 from oracle import oracle as O  # noqa: E402
-from recon_b200 import (FP_COLUMN_BLOCKS, FP_COLUMNS, PROJECTOR_FORWARD, SINO_BF16, SINO_F32, Options,  # noqa: E402
-                        Plan, ReconError)
+from recon_b200 import (FP_COLUMN_BLOCKS, FP_COLUMNS, PROJECTOR_FORWARD, SIDDON_BP_GATHER, SIDDON_BP_RAY,  # noqa: E402
+                        SINO_BF16, SINO_F32, Options, Plan, ReconError)
 from recon_b200.configs import geom_dict  # noqa: E402
 
 GEOMS = {
@@ -69,11 +69,14 @@ def test_blocked_projection(name):
     assert torch.equal(part.view(torch.int32), sb[3:8].view(torch.int32))
 
 
+# with the gather on the mirror geometry the ratio is kept in mirrored row pairs
+# (column_finish_pairs_kernel forms it from the block sums)
+@pytest.mark.parametrize("design", [SIDDON_BP_GATHER, SIDDON_BP_RAY])
 @pytest.mark.parametrize("sino", [SINO_F32, SINO_BF16])
 @pytest.mark.parametrize("name", ["mirror", "offset"])
-def test_blocked_mlem_iteration(name, sino):
+def test_blocked_mlem_iteration(name, sino, design):
     cfg, side, _ = GEOMS[name]
-    B, U = _plans(cfg, side, sino=sino)
+    B, U = _plans(cfg, side, sino=sino, siddon_bp=design)
     assert B.forward_projector == FP_COLUMN_BLOCKS
     vol = _volume(B, 72) + 0.2
     g = U.fp_views(vol)
