@@ -970,7 +970,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_pairs_kernel(
 // Dynamic shared memory: the rows' z planes (Nv float4), then the epilogue's
 // staging area [warp][d_r][lower voxels, mirrors][PS * 32].
 template <int EPI, class ST, int PS>
-__global__ void __launch_bounds__(kGatherWarps * 32, 2) bp_gather_quarter_kernel(
+__global__ void __launch_bounds__(kGatherWarps * 32, PS <= 2 ? 3 : 2) bp_gather_quarter_kernel(
     ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
     const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned nview, const ST* __restrict__ vals,
     size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens, unsigned long long* __restrict__ npairs)
@@ -2045,9 +2045,6 @@ static recon_status_t launch_gather_slots(Plan& P, const ST* vals, size_t view_s
                                           unsigned long long* npairs = nullptr)
 {
     const ExactGeom& E = P.eg;
-    if constexpr (MIRROR)
-        if (quarter_gather_serves<SLOTS>(P, first, count))
-            return launch_gather_quarter<EPI, ST, SLOTS>(P, vals, view_stride, vol, sens, s, npairs);
     const exact::GatherConst C = gather_const(P, vol, sens);
     const size_t smem = (size_t)E.Nv * sizeof(float4);
     auto kernel = [&P] {
@@ -2085,12 +2082,31 @@ int gather_mirror_slots(int Z)
     return std::min(4, std::max(1, (half + 32 * chunks - 1) / (32 * chunks)));
 }
 
+// Voxel pairs per lane for the quarter-turn kernel: the lower half's height
+// in as few chunks of at most kQuarterSlots x 32 slices as possible, split
+// evenly.
+constexpr int kQuarterSlots = 4;
+static int gather_quarter_slots(int Z)
+{
+    const int half = Z / 2;
+    const int chunks = (half + 32 * kQuarterSlots - 1) / (32 * kQuarterSlots);
+    return std::min(kQuarterSlots, std::max(1, (half + 32 * chunks - 1) / (32 * chunks)));
+}
+
 template <int EPI, class ST>
 static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride, unsigned first, unsigned count,
                                     float* vol, const float* sens, cudaStream_t s,
                                     unsigned long long* npairs = nullptr)
 {
     if (P.z_mirror) {
+        if (quarter_gather_serves<kQuarterSlots>(P, first, count)) {
+            switch (gather_quarter_slots(P.eg.Z)) {
+                case 1: return launch_gather_quarter<EPI, ST, 1>(P, vals, view_stride, vol, sens, s, npairs);
+                case 2: return launch_gather_quarter<EPI, ST, 2>(P, vals, view_stride, vol, sens, s, npairs);
+                case 3: return launch_gather_quarter<EPI, ST, 3>(P, vals, view_stride, vol, sens, s, npairs);
+                default: return launch_gather_quarter<EPI, ST, 4>(P, vals, view_stride, vol, sens, s, npairs);
+            }
+        }
         switch (gather_mirror_slots(P.eg.Z)) {
             case 1: return launch_gather_slots<EPI, ST, 1, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);
             case 2: return launch_gather_slots<EPI, ST, 2, true>(P, vals, view_stride, first, count, vol, sens, s, npairs);
