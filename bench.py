@@ -804,6 +804,7 @@ def main():
         "ratio_layout": ("mirrored row pairs" if gather and mirror and columns and P.nv % 2 == 0 else
                          "detector columns" if gather else "rows"),
         "mirror_pairs": mirror,
+        "quarter_turns": P.quarter_turns,
     }
     peaks = {}
     try:
@@ -822,7 +823,8 @@ def main():
             # mirrored row pairs where both projectors pair rows (even detector height,
             # detector-column forward projector)
             pairs = mirror and columns and P.nv % 2 == 0
-            dom = (("back projection (bp_gather_pairs_kernel)" if pairs else
+            dom = (("back projection (bp_gather_quarter_kernel)" if pairs and P.quarter_turns else
+                    "back projection (bp_gather_pairs_kernel)" if pairs else
                     "back projection (bp_gather_mirror_kernel)" if mirror else "back projection (bp_gather_kernel)")
                    if gather else
                    "back projection (maxabs + bp_ray_kernel per z-slab + bp_finish_kernel)", t_bp, bytes_bp,
@@ -835,6 +837,11 @@ def main():
                            "frac": ach / hbm, "peak_source": peak_src, "traffic": dom[3],
                            "traffic_source": TRAFFIC_PROFILE if dom[3] is not None else None,
                            "algorithmic_bytes_per_launch": dom[2], "launch_ms": dom[1]}
+        if dom[3] is not None:
+            # the DRAM bytes the kernel moves (ncu): most algorithmic bytes (4 per
+            # intersection) are served from L1 / L2, so frac can pass 1 while DRAM idles
+            out["roofline"]["dram_achieved"] = dom[3] / (dom[1] * 1e-3) / 1e9
+            out["roofline"]["dram_frac"] = out["roofline"]["dram_achieved"] / hbm
         b_iter = 8.0 * isects + 4.0 * npix * nviews + 12.0 * nvox
         b_comp = 4.0 * npix * nviews + 12.0 * nvox  # the bytes no design avoids: g once, f and sens read, f written
         out["iteration_roofline"] = {"bytes_per_iteration": b_iter, "achieved_gbs": b_iter / (ms_step * 1e-3) / 1e9,
