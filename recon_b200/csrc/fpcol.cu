@@ -216,10 +216,9 @@ __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ vol
 {
     int dm = Z + 1 - 2 * kaddr;  // the mirror row's offset from row v's in the same column
     float acc = 0.0f, comp = 0.0f, accm = 0.0f, compm = 0.0f, f1 = 0.0f, f1m = 0.0f;
-    auto piece = [&](int j, float& blk, float& blkm) {
-        const float2 pc = spc[j];
-        const float B = pc.x;
-        const int cb = __float_as_int(pc.y);
+    // piece {B, column}: B = where it ends, its column's offset in volz (int bits)
+    auto piece_at = [&](float B, float cbits, float& blk, float& blkm) {
+        const int cb = __float_as_int(cbits);
         const float* p = volz + (cb + kaddr);
         const float* pm = p + dm;
         const bool cross = tzn < B;
@@ -250,12 +249,33 @@ __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ vol
         }
         cur = B;
     };
+    auto piece = [&](int j, float& blk, float& blkm) {
+        const float2 pc = spc[j];
+        piece_at(pc.x, pc.y, blk, blkm);
+    };
+    const float4* spc4 = reinterpret_cast<const float4*>(spc);  // pieces 2i, 2i + 1
     int j = jb;
-    // blocks of 16 pieces: the pair's loads of a block issue together
+    // blocks of 16 pieces: the pair's loads of a block issue together; the
+    // table is read two pieces per 16-byte load (j is the same for the warp)
     for (; j + 15 <= je; j += 16) {
         float blk = 0.0f, blkm = 0.0f;
+        if ((j & 1) == 0) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) piece(j + q, blk, blkm);
+            for (int q = 0; q < 8; ++q) {
+                const float4 pp = spc4[(j >> 1) + q];
+                piece_at(pp.x, pp.y, blk, blkm);
+                piece_at(pp.z, pp.w, blk, blkm);
+            }
+        } else {
+            piece(j, blk, blkm);
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const float4 pp = spc4[((j + 1) >> 1) + q];
+                piece_at(pp.x, pp.y, blk, blkm);
+                piece_at(pp.z, pp.w, blk, blkm);
+            }
+            piece(j + 15, blk, blkm);
+        }
         if (KAHAN && !COUNT) {
             kahan_add(acc, comp, blk);
             kahan_add(accm, compm, blkm);
@@ -341,7 +361,7 @@ __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, cons
 // MIRROR: rows come in mirrored pairs (see walk_rows_mirror); the CTA's rows
 // are lower rows (below Nv/2) and each lane also produces its mirror row.
 template <bool KAHAN, int MODE, int LAYOUT, class GT, class OT, bool MIRROR = false>
-__global__ void __launch_bounds__(kColRows) fp_column_kernel(ExactGeom G, const float4* __restrict__ txy,
+__global__ void __launch_bounds__(kColRows, 16) fp_column_kernel(ExactGeom G, const float4* __restrict__ txy,
                                                              const int2* __restrict__ kxy,
                                                              const ZParam* __restrict__ zp,
                                                              const float* __restrict__ wq,
