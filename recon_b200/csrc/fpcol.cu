@@ -210,7 +210,7 @@ __device__ __forceinline__ float column_row_sum(const ExactGeom& G, const ZParam
 // test and plane update, two loads and two sums.  The mirror's layer is
 // Z-1-k, at offset Z + 1 - kaddr of its padded column.  Returns {row v, row
 // Nv-1-v}.
-template <bool KAHAN, bool FAST, bool COUNT>
+template <bool KAHAN, bool FAST, bool COUNT, bool PAIRED>
 __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ volz, const float2* spc, int jb, int je,
                                                    float cur, int kaddr, float kf, float tzn, float S, float O, int Z)
 {
@@ -255,11 +255,15 @@ __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ vol
     };
     const float4* spc4 = reinterpret_cast<const float4*>(spc);  // pieces 2i, 2i + 1
     int j = jb;
-    // blocks of 16 pieces: the pair's loads of a block issue together; the
-    // table is read two pieces per 16-byte load (j is the same for the warp)
+    // blocks of 16 pieces: the pair's loads of a block issue together; with
+    // PAIRED the table is read two pieces per 16-byte load (j is the same for
+    // the warp)
     for (; j + 15 <= je; j += 16) {
         float blk = 0.0f, blkm = 0.0f;
-        if ((j & 1) == 0) {
+        if (!PAIRED) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) piece(j + q, blk, blkm);
+        } else if ((j & 1) == 0) {
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const float4 pp = spc4[(j >> 1) + q];
@@ -296,7 +300,7 @@ __device__ __forceinline__ float2 walk_rows_mirror(const float* __restrict__ vol
 }
 
 // column_row_sum for lower row v (v < Nv/2) and its mirror Nv-1-v.
-template <bool KAHAN, bool COUNT>
+template <bool KAHAN, bool COUNT, bool PAIRED>
 __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, const ZParam* __restrict__ zp,
                                                         const float* __restrict__ volz, const float2* spc, int n,
                                                         float t_in, float t_out, int v, bool valid)
@@ -339,8 +343,9 @@ __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, cons
     }
     const bool leaves = hit && t_start < t_hi && t_end > t_hi;
     if (!__any_sync(0xffffffffu, leaves))
-        return walk_rows_mirror<KAHAN, true, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, G.Z);
-    return walk_rows_mirror<KAHAN, false, COUNT>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, G.Z);
+        return walk_rows_mirror<KAHAN, true, COUNT, PAIRED>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O,
+                                                            G.Z);
+    return walk_rows_mirror<KAHAN, false, COUNT, PAIRED>(volz, spc, jb, je, t_start, kaddr, kf, tzn, Z.S, Z.O, G.Z);
 }
 
 // MODE 0: out = projection (w * sum); MODE 1 (MLEM): out = w * g / Hf (0 where
@@ -361,13 +366,7 @@ __device__ __forceinline__ float2 column_row_sum_mirror(const ExactGeom& G, cons
 // MIRROR: rows come in mirrored pairs (see walk_rows_mirror); the CTA's rows
 // are lower rows (below Nv/2) and each lane also produces its mirror row.
 template <bool KAHAN, int MODE, int LAYOUT, class GT, class OT, bool MIRROR = false>
-__global__ void __launch_bounds__(kColRows, 16) fp_column_kernel(ExactGeom G, const float4* __restrict__ txy,
-                                                             const int2* __restrict__ kxy,
-                                                             const ZParam* __restrict__ zp,
-                                                             const float* __restrict__ wq,
-                                                             const uint2* __restrict__ tiles, unsigned view0,
-                                                             int4 blk, const float* __restrict__ volz,
-                                                             const GT* __restrict__ g, OT* __restrict__ out)
+__device__ __forceinline__ void column_kernel_body(ExactGeom G, const float4* __restrict__ txy, const int2* __restrict__ kxy, const ZParam* __restrict__ zp, const float* __restrict__ wq, const uint2* __restrict__ tiles, unsigned view0, int4 blk, const float* __restrict__ volz, const GT* __restrict__ g, OT* __restrict__ out)
 {
     // piece j: {t where it ends, offset of its (x, y) voxel column in volz (int bits)}
     extern __shared__ float2 spc[];
@@ -439,7 +438,9 @@ __global__ void __launch_bounds__(kColRows, 16) fp_column_kernel(ExactGeom G, co
     const bool valid = v < vend;
     float2 sum = make_float2(0.0f, 0.0f);
     if (n > 0) {
-        if (MIRROR) sum = column_row_sum_mirror<KAHAN, COUNTING>(G, zp, volz, spc, n, t_in, t_out, v, valid);
+        // the table read in pairs for whole-volume walks; the xy blocks' shorter
+        // walks measured faster reading it piece by piece
+        if (MIRROR) sum = column_row_sum_mirror<KAHAN, COUNTING, (MODE < 4)>(G, zp, volz, spc, n, t_in, t_out, v, valid);
         else sum.x = column_row_sum<KAHAN, COUNTING>(G, zp, volz, spc, n, t_in, t_out, v, valid);
     }
     if (COUNTING) {
@@ -481,6 +482,27 @@ __global__ void __launch_bounds__(kColRows, 16) fp_column_kernel(ExactGeom G, co
             if (MIRROR) emit(G.Nv - 1 - v, sum.y);
         }
     }
+}
+
+// The whole-volume walks (MODES 0 .. 3) held at 32 registers, 16 CTAs per SM:
+// 2.98 against 3.07 ms at 256^3 / 360 / 512^2.  The xy-block walks (MODES 4, 5)
+// keep the compiler's own allocation, which measured faster for them.
+template <bool KAHAN, int MODE, int LAYOUT, class GT, class OT, bool MIRROR = false>
+__global__ void __launch_bounds__(kColRows, 16) fp_column_kernel(ExactGeom G, const float4* __restrict__ txy, const int2* __restrict__ kxy, const ZParam* __restrict__ zp, const float* __restrict__ wq, const uint2* __restrict__ tiles, unsigned view0, int4 blk, const float* __restrict__ volz, const GT* __restrict__ g, OT* __restrict__ out)
+{
+    column_kernel_body<KAHAN, MODE, LAYOUT, GT, OT, MIRROR>(G, txy, kxy, zp, wq, tiles, view0, blk, volz, g, out);
+}
+template <bool KAHAN, int MODE, int LAYOUT, class GT, class OT, bool MIRROR = false>
+__global__ void __launch_bounds__(kColRows) fp_column_block_kernel(ExactGeom G, const float4* __restrict__ txy, const int2* __restrict__ kxy, const ZParam* __restrict__ zp, const float* __restrict__ wq, const uint2* __restrict__ tiles, unsigned view0, int4 blk, const float* __restrict__ volz, const GT* __restrict__ g, OT* __restrict__ out)
+{
+    column_kernel_body<KAHAN, MODE, LAYOUT, GT, OT, MIRROR>(G, txy, kxy, zp, wq, tiles, view0, blk, volz, g, out);
+}
+// the kernel of a MODE
+template <int MODE, bool KAHAN, int LAYOUT, class GT, class OT, bool MIRROR>
+constexpr auto fp_column_kernel_of()
+{
+    if constexpr (MODE >= 4) return fp_column_block_kernel<KAHAN, MODE, LAYOUT, GT, OT, MIRROR>;
+    else return fp_column_kernel<KAHAN, MODE, LAYOUT, GT, OT, MIRROR>;
 }
 
 // f[z][y][x] -> volz[(y*X + x)*(Z + 2) + z + 1], 32 (x) x 32 (z) tiles of one y
@@ -785,13 +807,13 @@ static auto column_kernel(const Plan& P)
 {
     const bool kahan = P.opt.sum == RECON_SUM_KAHAN;
     if constexpr (LAYOUT == kLayoutPairs) {  // only from the mirror-paired walk
-        return kahan ? exact::fp_column_kernel<true, MODE, LAYOUT, GT, OT, true>
-                     : exact::fp_column_kernel<false, MODE, LAYOUT, GT, OT, true>;
+        return kahan ? exact::fp_column_kernel_of<MODE, true, LAYOUT, GT, OT, true>()
+                     : exact::fp_column_kernel_of<MODE, false, LAYOUT, GT, OT, true>();
     } else {
-        return P.z_mirror ? (kahan ? exact::fp_column_kernel<true, MODE, LAYOUT, GT, OT, true>
-                                   : exact::fp_column_kernel<false, MODE, LAYOUT, GT, OT, true>)
-                          : (kahan ? exact::fp_column_kernel<true, MODE, LAYOUT, GT, OT, false>
-                                   : exact::fp_column_kernel<false, MODE, LAYOUT, GT, OT, false>);
+        return P.z_mirror ? (kahan ? exact::fp_column_kernel_of<MODE, true, LAYOUT, GT, OT, true>()
+                                   : exact::fp_column_kernel_of<MODE, false, LAYOUT, GT, OT, true>())
+                          : (kahan ? exact::fp_column_kernel_of<MODE, true, LAYOUT, GT, OT, false>()
+                                   : exact::fp_column_kernel_of<MODE, false, LAYOUT, GT, OT, false>());
     }
 }
 
