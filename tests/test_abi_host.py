@@ -193,3 +193,14 @@ def test_elementwise_argument_checks():
     assert lib.recon_set_ones(None, 0, None) == 0
     assert lib.recon_set_ones(None, 5, None) == 1
     assert lib.recon_divide1(None, None, 3, None) == 1
+
+
+def test_plan_queries_reject_null():
+    """The plan queries refuse a NULL plan or output before touching either."""
+    lib = L.lib()
+    out = C.c_int(-7)
+    for name in ("recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_plan_mirror_pairs",
+                 "recon_plan_quarter_turns", "recon_plan_column_rows"):
+        fn = getattr(lib, name)
+        assert fn(None, C.byref(out)) == 1, name
+        assert out.value == -7, name
