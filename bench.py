@@ -658,7 +658,12 @@ def main():
     P.mlem_prepare()
     f = P.new_volume(1.0)
     ht = P.new_volume(0.0)
-    first, count = view_range(nviews, rank, world)
+    if P.quarter_sets:  # a rank's views: the same base range of each quarter (sharded_mlem_iteration)
+        qf, qc = view_range(nviews // 4, rank, world)
+        ranges = [(qf + r * (nviews // 4), qc) for r in range(4)]
+    else:
+        ranges = [view_range(nviews, rank, world)]
+    count = sum(c for _, c in ranges)
     npix = P.nu * P.nv
     nvox = f.numel()
     # kernels per step: the volume's copy (z-fastest for the column forward
@@ -727,7 +732,7 @@ def main():
         h2d = [0]
 
         def e2e_sharded():
-            h2d[0] = P.upload_sinogram(g_host, g, first, count)
+            h2d[0] = sum(P.upload_sinogram(g_host, g, a, c) for a, c in ranges)
             iteration()
             if rank == 0:
                 f_host.copy_(f, non_blocking=True)

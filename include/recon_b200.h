@@ -218,7 +218,9 @@ recon_status_t recon_plan_mirror_pairs(recon_plan_t plan, int* paired);
  * quarter's by exact quarter turns, so both projectors give column (x, y) at
  * view n + NumProj/4 exactly the lengths of column (Xdim-1-y, x) at view n,
  * and the mirror-paired gather back projector finds each set of lengths once
- * for four columns.  No counterpart in the reference. */
+ * for four columns.  *quarter = 2 when, besides, that gather is the plan's
+ * MLEM back projector, so recon_mlem_backward_quarters serves it.  0
+ * otherwise.  No counterpart in the reference. */
 recon_status_t recon_plan_quarter_turns(recon_plan_t plan, int* quarter);
 /* *rows = the detector rows per CTA of the plan's detector-column forward
  * projector (32, 64 or 128: the fewest that cover a column's rows, or the
@@ -320,6 +322,20 @@ recon_status_t recon_mlem_forward(recon_plan_t plan, const void* d_g, const floa
 recon_status_t recon_mlem_backward(recon_plan_t plan, unsigned int first, unsigned int count,
                                    float* d_ht, void* stream);
 recon_status_t recon_mlem_update(recon_plan_t plan, float* d_f, const float* d_ht, void* stream);
+/* The two halves over a quarter set of views: views first .. first+count-1
+ * and the same views of the other three quarters (view n + k*NumProj/4,
+ * k = 1, 2, 3), first + count <= NumProj/4, for plans whose views come in
+ * quarter turns (recon_plan_quarter_turns).  A split of the views between
+ * devices by quarter sets keeps the quarter-turn gather on every device,
+ * where a split into contiguous view ranges gives it up.  forward: as
+ * recon_mlem_forward over the four ranges (d_g holds all NumProj views);
+ * backward: d_ht = sum over the set of BP(ratio) (overwritten), plans with
+ * recon_plan_quarter_turns = 2 only (RECON_ERR_UNSUPPORTED otherwise).  No
+ * counterpart in the reference. */
+recon_status_t recon_mlem_forward_quarters(recon_plan_t plan, const void* d_g, const float* d_f,
+                                           unsigned int first, unsigned int count, void* stream);
+recon_status_t recon_mlem_backward_quarters(recon_plan_t plan, unsigned int first, unsigned int count,
+                                            float* d_ht, void* stream);
 /* backward over all views with the update fused into it (no Ht buffer):
  * recon_mlem_forward(all views) followed by this is one recon_mlem_iteration. */
 recon_status_t recon_mlem_backward_update(recon_plan_t plan, float* d_f, void* stream);

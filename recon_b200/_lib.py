@@ -122,6 +122,8 @@ def lib() -> C.CDLL:
         "recon_mlem_forward": (st, [P, P, P, u, u, P]),
         "recon_mlem_backward": (st, [P, u, u, P, P]),
         "recon_mlem_update": (st, [P, P, P, P]),
+        "recon_mlem_forward_quarters": (st, [P, P, P, u, u, P]),
+        "recon_mlem_backward_quarters": (st, [P, u, u, P, P]),
         "recon_mlem_backward_update": (st, [P, P, P]),
         "recon_count_intersections": (st, [P, C.POINTER(C.c_ulonglong)]),
         "recon_count_projector_pairs": (st, [P, C.c_int, C.POINTER(C.c_ulonglong)]),
@@ -157,7 +159,7 @@ def exported_symbols() -> list[str]:
         "recon_plan_create", "recon_plan_destroy", "recon_plan_device_bytes", "recon_plan_siddon_bp", "recon_plan_forward_projector", "recon_plan_mirror_pairs", "recon_plan_quarter_turns", "recon_plan_column_rows", "recon_fp_view", "recon_fp_views",
         "recon_bp_view", "recon_bp_views", "recon_sensitivity", "recon_voxel_bp_view", "recon_march_fp_view", "recon_mlem",
         "recon_mlem_prepare", "recon_mlem_iteration", "recon_mlem_forward", "recon_mlem_backward",
-        "recon_mlem_update", "recon_mlem_backward_update", "recon_count_intersections", "recon_count_projector_pairs", "recon_set_ones", "recon_divide1", "recon_multiply1",
+        "recon_mlem_update", "recon_mlem_forward_quarters", "recon_mlem_backward_quarters", "recon_mlem_backward_update", "recon_count_intersections", "recon_count_projector_pairs", "recon_set_ones", "recon_divide1", "recon_multiply1",
         "recon_add", "recon_compat_setup_view", "recon_compat_trace", "recon_view_step_count", "recon_mlem_from_cfg",
         "recon_forward_projection_from_cfg", "recon_backward_projection_from_cfg", "recon_batch_create",
         "recon_batch_destroy", "recon_batch_mlem", "recon_compat_bp_view_noalloc", "recon_osem",

@@ -153,9 +153,18 @@ class Plan:
     @property
     def quarter_turns(self) -> bool:
         """True when an EXACT plan's views come in exact quarter turns about a square volume."""
+        return self._quarter_level() >= 1
+
+    @property
+    def quarter_sets(self) -> bool:
+        """True when the MLEM back projection also takes quarter sets of views
+        (recon_mlem_backward_quarters): recon_plan_quarter_turns reports 2."""
+        return self._quarter_level() == 2
+
+    def _quarter_level(self) -> int:
         d = C.c_int(0)
         check(lib().recon_plan_quarter_turns(self._h, C.byref(d)))
-        return bool(d.value)
+        return int(d.value)
 
     @property
     def forward_projector(self) -> int:
@@ -262,6 +271,14 @@ class Plan:
     def mlem_backward(self, ht, first: int = 0, count: int | None = None) -> None:
         count = self.nproj - first if count is None else count
         check(lib().recon_mlem_backward(self._h, first, count, _ptr(ht), _stream()))
+
+    def mlem_forward_quarters(self, g, f, first: int, count: int) -> None:
+        """recon_mlem_forward_quarters: the ratio of base views first .. first+count-1 of each quarter."""
+        check(lib().recon_mlem_forward_quarters(self._h, _ptr(g), _ptr(f), first, count, _stream()))
+
+    def mlem_backward_quarters(self, ht, first: int, count: int) -> None:
+        """recon_mlem_backward_quarters: ht = the back projection of that quarter set's ratio."""
+        check(lib().recon_mlem_backward_quarters(self._h, first, count, _ptr(ht), _stream()))
 
     def mlem_update(self, f, ht) -> None:
         check(lib().recon_mlem_update(self._h, _ptr(f), _ptr(ht), _stream()))

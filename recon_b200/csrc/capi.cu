@@ -375,7 +375,7 @@ recon_status_t recon_plan_mirror_pairs(recon_plan_t plan, int* paired)
 recon_status_t recon_plan_quarter_turns(recon_plan_t plan, int* quarter)
 {
     if (!plan || !quarter) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
-    *quarter = (plan->opt.arith == RECON_ARITH_EXACT && plan->quarter) ? 1 : 0;
+    *quarter = (plan->opt.arith == RECON_ARITH_EXACT && plan->quarter) ? (exact_quarter_sets(*plan) ? 2 : 1) : 0;
     return RECON_OK;
 }
 
@@ -561,6 +561,37 @@ recon_status_t recon_mlem_backward(recon_plan_t P, unsigned first, unsigned coun
     const void* r = static_cast<const char*>(P->d_ratio) + (size_t)first * column_view_elems(*P) * es;
     return exact_bp(*P, r, true, P->opt.sino == RECON_SINO_BF16, first, count, false, false, d_ht, nullptr, nullptr,
                     s);
+}
+
+// Quarter sets: base views first .. first + count - 1 (first + count <= N/4) and
+// their turns by one, two and three quarters.
+static recon_status_t quarters_ok(recon_plan_t P, unsigned first, unsigned count)
+{
+    RB_CHECK(split_ok(P, 0, P ? P->nviews : 0));
+    if (!P->quarter) return fail(RECON_ERR_UNSUPPORTED, "the plan's views do not come in quarter turns");
+    if ((size_t)first + count > P->nviews / 4) return fail(RECON_ERR_INVALID_ARGUMENT, "quarter range beyond NumProj/4");
+    return RECON_OK;
+}
+
+recon_status_t recon_mlem_forward_quarters(recon_plan_t P, const void* d_g, const float* d_f, unsigned first,
+                                           unsigned count, void* stream)
+{
+    RB_CHECK(quarters_ok(P, first, count));
+    if (!d_g || !d_f) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    RB_CHECK(use_device(*P));
+    const unsigned q = P->nviews / 4;
+    for (unsigned r = 0; r < 4 && count > 0; ++r)
+        RB_CHECK(exact_fp_ratio(*P, d_f, d_g, P->d_ratio, as_stream(stream), first + r * q, count));
+    return RECON_OK;
+}
+
+recon_status_t recon_mlem_backward_quarters(recon_plan_t P, unsigned first, unsigned count, float* d_ht,
+                                            void* stream)
+{
+    RB_CHECK(quarters_ok(P, first, count));
+    if (!d_ht) return fail(RECON_ERR_INVALID_ARGUMENT, "NULL argument");
+    RB_CHECK(use_device(*P));
+    return exact_bp_quarters(*P, first, count, d_ht, as_stream(stream));
 }
 
 recon_status_t recon_mlem_update(recon_plan_t P, float* d_f, const float* d_ht, void* stream)

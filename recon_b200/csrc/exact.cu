@@ -953,8 +953,9 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_pairs_kernel(
 }
 
 
-// The pair gather over all of a plan's views where views a quarter turn apart
-// are exact rotations of each other (Plan::quarter, tables from
+// The pair gather over a quarter set of a plan's views (base views m0 .. m0 +
+// mc - 1 and their turns by one, two and three quarters; all views for m0 = 0,
+// mc = N/4) where views a quarter turn apart are exact rotations of each other (Plan::quarter, tables from
 // quarter_turn_table_kernel: N = 4Q views, column c at view n + Q is column
 // rho(c) = (X-1-j, i) at view n, bit for bit).  The candidate rows and lengths
 // found for base column c0 = (i, j) at view m therefore serve the four columns
@@ -963,17 +964,19 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_pairs_kernel(
 // (d_r = rho^-r(c0)) at views m, m + Q, m + 2Q, m + 3Q (mod N): a lane finds a
 // voxel pair's rows and lengths once and loads four value pairs for them, one
 // per view.  Base columns tile the quadrant i, j < X/2 (one orbit each); a
-// CTA's 4 x 2 base columns are 8 warps as in bp_gather_pairs_kernel.  Column
-// d_r sums its views in the order rQ .. N-1, 0 .. rQ-1, each piece's further
-// candidate rows after its first ones, into the same registers: deterministic,
-// the same lengths as bp_gather_pairs_kernel, the sums in another order.
+// CTA's 4 x 2 base columns are 8 warps as in bp_gather_pairs_kernel.  Over all
+// views column d_r sums its views in the order rQ .. N-1, 0 .. rQ-1, each
+// piece's further candidate rows after its first ones, into the same
+// registers: deterministic, the same lengths as bp_gather_pairs_kernel, the
+// sums in another order.
 // Dynamic shared memory: the rows' z planes (Nv float4), then the epilogue's
 // staging area [warp][d_r][lower voxels, mirrors][PS * 32].
 template <int EPI, class ST, int PS>
 __global__ void __launch_bounds__(kGatherWarps * 32, PS <= 2 ? 3 : 2) bp_gather_quarter_kernel(
     ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
-    const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned nview, const ST* __restrict__ vals,
-    size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens, unsigned long long* __restrict__ npairs)
+    const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned nview, unsigned m0, unsigned mc,
+    const ST* __restrict__ vals, size_t view_stride, float* __restrict__ vol, const float* __restrict__ sens,
+    unsigned long long* __restrict__ npairs)
 {
     extern __shared__ float4 szq[];
     __shared__ GatherView sview[kGatherWarps][32];
@@ -990,8 +993,12 @@ __global__ void __launch_bounds__(kGatherWarps * 32, PS <= 2 ? 3 : 2) bp_gather_
     const int i0 = blockIdx.x * kGatherTileX, j0 = blockIdx.y * (kGatherWarps / kGatherTileX);
     const int i = i0 + warp % kGatherTileX, j = j0 + warp / kGatherTileX;
     const bool active = i < H && j < H;
-    const unsigned nview_w = active ? nview : 0u;
     const unsigned Q = nview / 4u;
+    // the views summed: base views m0 .. m0 + mc - 1 of each quarter (all views
+    // for m0 = 0, mc = Q), item i being view m0 + i % mc + (i / mc) Q; the set is
+    // closed under quarter turns, so every turned column gets the same views
+    const unsigned nview_w = active ? 4u * mc : 0u;
+    auto view_of = [&](unsigned it) { return m0 + it % mc + (it / mc) * Q; };
     GatherView* sv = sview[warp];
     const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
     const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
@@ -1100,10 +1107,11 @@ __global__ void __launch_bounds__(kGatherWarps * 32, PS <= 2 ? 3 : 2) bp_gather_
         for (unsigned vb = 0; vb < nview_w; vb += 32) {
             const unsigned nb = min(32u, nview_w - vb);
             if ((unsigned)lane < nb)  // lane q sets up view vb + q
-                sv[lane] = gather_view(G, C, txy, kxy, cs, vb + lane, i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo, dz32);
+                sv[lane] = gather_view(G, C, txy, kxy, cs, view_of(vb + lane), i, j, Xa, Xb, Ya, Yb, oz_hi - oz_lo,
+                                       dz32);
             __syncwarp();
             for (unsigned q = 0; q < nb; ++q) {
-                const unsigned m = vb + q;
+                const unsigned m = view_of(vb + q);
                 const ST* vm[4];  // views m + rQ (mod N) from detector column 0
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
@@ -2018,9 +2026,19 @@ static bool quarter_gather_serves(const Plan& P, unsigned first, unsigned count)
            quarter_dynamic_smem<PS>(P) + kQuarterStaticSmem <= 227 * 1024;
 }
 
+// The plan's MLEM back projection takes quarter sets of views
+// (exact_bp_quarters): the quarter-turn gather is its back projector.
+bool exact_quarter_sets(const Plan& P)
+{
+    return P.opt.arith == RECON_ARITH_EXACT && P.opt.bp == RECON_BP_SIDDON && P.bp_gather &&
+           quarter_gather_serves<4>(P, 0, P.nviews);
+}
+
+// vals: view 0 of the plan's views; m0, mc: the base views of the quarter set
 template <int EPI, class ST, int PS>
 static recon_status_t launch_gather_quarter(Plan& P, const ST* vals, size_t view_stride, float* vol,
-                                            const float* sens, cudaStream_t s, unsigned long long* npairs)
+                                            const float* sens, cudaStream_t s, unsigned long long* npairs,
+                                            unsigned m0, unsigned mc)
 {
     const ExactGeom& E = P.eg;
     const exact::GatherConst C = gather_const(P, vol, sens);
@@ -2031,8 +2049,8 @@ static recon_status_t launch_gather_quarter(Plan& P, const ST* vals, size_t view
     constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
     const int H = E.X / 2;  // base columns: the quadrant x, y < X/2
     const dim3 grid((H + tx - 1) / tx, (H + ty - 1) / ty);
-    kernel<<<grid, exact::kGatherWarps * 32, smem, s>>>(E, C, P.d_txy, P.d_kxy, P.d_cs, P.d_zp, P.nviews, vals,
-                                                         view_stride, vol, sens, npairs);
+    kernel<<<grid, exact::kGatherWarps * 32, smem, s>>>(E, C, P.d_txy, P.d_kxy, P.d_cs, P.d_zp, P.nviews, m0, mc,
+                                                         vals, view_stride, vol, sens, npairs);
     RB_CUDA(cudaGetLastError());
     return RECON_OK;
 }
@@ -2100,11 +2118,12 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
 {
     if (P.z_mirror) {
         if (quarter_gather_serves<kQuarterSlots>(P, first, count)) {
+            const unsigned q = P.nviews / 4;
             switch (gather_quarter_slots(P.eg.Z)) {
-                case 1: return launch_gather_quarter<EPI, ST, 1>(P, vals, view_stride, vol, sens, s, npairs);
-                case 2: return launch_gather_quarter<EPI, ST, 2>(P, vals, view_stride, vol, sens, s, npairs);
-                case 3: return launch_gather_quarter<EPI, ST, 3>(P, vals, view_stride, vol, sens, s, npairs);
-                default: return launch_gather_quarter<EPI, ST, 4>(P, vals, view_stride, vol, sens, s, npairs);
+                case 1: return launch_gather_quarter<EPI, ST, 1>(P, vals, view_stride, vol, sens, s, npairs, 0u, q);
+                case 2: return launch_gather_quarter<EPI, ST, 2>(P, vals, view_stride, vol, sens, s, npairs, 0u, q);
+                case 3: return launch_gather_quarter<EPI, ST, 3>(P, vals, view_stride, vol, sens, s, npairs, 0u, q);
+                default: return launch_gather_quarter<EPI, ST, 4>(P, vals, view_stride, vol, sens, s, npairs, 0u, q);
             }
         }
         switch (gather_mirror_slots(P.eg.Z)) {
@@ -2127,6 +2146,29 @@ static recon_status_t launch_gather(Plan& P, const ST* vals, size_t view_stride,
         default: return launch_gather_slots<EPI, ST, 8>(P, vals, view_stride, first, count, vol, sens, s, npairs);
     }
 #undef RB_GATHER_SLOTS
+}
+
+// The MLEM ratio's back projection over the quarter set of base views first ..
+// first + count - 1 (first + count <= N/4) and their quarter turns, into vol
+// (overwritten); the plan takes quarter sets (exact_quarter_sets).
+recon_status_t exact_bp_quarters(Plan& P, unsigned first, unsigned count, float* vol, cudaStream_t s)
+{
+    if (!exact_quarter_sets(P)) return fail(RECON_ERR_UNSUPPORTED, "the plan's back projection takes no quarter sets");
+    if ((size_t)first + count > P.nviews / 4) return fail(RECON_ERR_INVALID_ARGUMENT, "quarter range beyond NumProj/4");
+    if (count == 0) return launch_fill(vol, 0.0f, P.nvox, s);
+    const size_t qv = column_view_elems(P);
+    auto run = [&](auto tag) -> recon_status_t {
+        using ST = decltype(tag);
+        const ST* vals = static_cast<const ST*>(P.d_ratio);
+        switch (gather_quarter_slots(P.eg.Z)) {
+            case 1: return launch_gather_quarter<0, ST, 1>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+            case 2: return launch_gather_quarter<0, ST, 2>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+            case 3: return launch_gather_quarter<0, ST, 3>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+            default: return launch_gather_quarter<0, ST, 4>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+        }
+    };
+    if (P.opt.sino == RECON_SINO_BF16) return run(__nv_bfloat16{});
+    return run(float{});
 }
 
 // (ray, voxel) pairs the gather back projector gives a positive length, over

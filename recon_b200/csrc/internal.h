@@ -254,6 +254,8 @@ int gather_slots(int Z);
 // layout [view][u][v].
 bool mlem_ratio_in_columns(const Plan& P);
 recon_status_t build_exact_culling(Plan& P);
+bool exact_quarter_sets(const Plan& P);
+recon_status_t exact_bp_quarters(Plan& P, unsigned first, unsigned count, float* vol, cudaStream_t s);
 recon_status_t exact_check_mirror(Plan& P);
 recon_status_t exact_tune_bp(Plan& P);
 // forward projection by detector columns (fpcol.cu)

@@ -66,12 +66,21 @@ def sharded_mlem_iteration(P, g, f, ht, group=None) -> None:
     `group`: P.mlem_forward / mlem_backward over this rank's views (the C ABI's
     recon_mlem_forward / recon_mlem_backward), the rank-ordered sum of the
     partial images, then P.mlem_update (recon_mlem_update) on every rank.  P is
-    any object with those three methods and `nproj`."""
+    any object with those three methods and `nproj`.  Where P.quarter_sets, a
+    rank's views are a quarter set (the same range of base views in each of the
+    four quarters, recon_mlem_forward_quarters / recon_mlem_backward_quarters)."""
     rank = dist.get_rank(group) if dist.is_initialized() else 0
     world = dist.get_world_size(group) if dist.is_initialized() else 1
-    first, count = view_range(P.nproj, rank, world)
-    P.mlem_forward(g, f, first, count)
-    P.mlem_backward(ht, first, count)
+    if getattr(P, "quarter_sets", False):
+        # views in quarter sets: the same base views of each quarter, so every
+        # rank keeps the gather that serves four views a quarter turn apart
+        first, count = view_range(P.nproj // 4, rank, world)
+        P.mlem_forward_quarters(g, f, first, count)
+        P.mlem_backward_quarters(ht, first, count)
+    else:
+        first, count = view_range(P.nproj, rank, world)
+        P.mlem_forward(g, f, first, count)
+        P.mlem_backward(ht, first, count)
     if world > 1:
         ordered_sum_(ht, group)
     P.mlem_update(f, ht)

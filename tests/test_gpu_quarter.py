@@ -164,3 +164,49 @@ def test_quarter_mlem(sino):
     assert fused.abs().sum().item() > 0
     assert torch.equal(fused.view(torch.int32), split.view(torch.int32))
     assert torch.equal(fused.view(torch.int32), again.view(torch.int32))  # deterministic
+
+
+@pytest.mark.parametrize("sino", ["f32", "bf16"])
+def test_quarter_sets(sino):
+    """recon_mlem_forward_quarters / recon_mlem_backward_quarters: the views of
+    ranks that split the plan by quarter sets (run one after another on this
+    GPU) sum to the back projection of all views (<= 1e-6: the sets' sums are
+    added at the end); the set of every base view is the all-views call, bit
+    for bit; plans without quarter turns refuse."""
+    from recon_b200 import ReconError
+    from recon_b200.sharding import view_range
+
+    cfg = small_cfg(NumProj=16, DeltaAng=22.5)
+    kw = {"sino": SINO_BF16} if sino == "bf16" else {}
+    P = Plan(cfg, Options(siddon_bp=SIDDON_BP_GATHER, **kw))
+    assert P.quarter_sets
+    gen = torch.Generator("cuda").manual_seed(105)
+    g = torch.rand((P.nproj, P.nv, P.nu), device="cuda", generator=gen) * 3
+    if sino == "bf16":
+        g = g.to(torch.bfloat16)
+    P.mlem_prepare()
+    f = torch.rand(P.shape_vol, device="cuda", generator=gen) + 0.5
+    P.mlem_forward(g, f)
+    whole = P.new_volume()
+    P.mlem_backward(whole)
+    q = P.nproj // 4
+    all_sets = P.new_volume()
+    P.mlem_forward_quarters(g, f, 0, q)
+    P.mlem_backward_quarters(all_sets, 0, q)
+    torch.cuda.synchronize()
+    assert torch.equal(whole.view(torch.int32), all_sets.view(torch.int32))
+    for world in (2, 3):
+        total = P.new_volume()
+        for rank in range(world):
+            first, count = view_range(q, rank, world)
+            part = P.new_volume(7.0)
+            P.mlem_forward_quarters(g, f, first, count)
+            P.mlem_backward_quarters(part, first, count)
+            total += part
+        torch.cuda.synchronize()
+        assert rel_l2(total.double().cpu().numpy(), whole.double().cpu().numpy()) < 1e-6, world
+    other = Plan(small_cfg(NumProj=10), Options(siddon_bp=SIDDON_BP_GATHER))
+    assert not other.quarter_turns and not other.quarter_sets
+    other.mlem_prepare()
+    with pytest.raises(ReconError):
+        other.mlem_backward_quarters(other.new_volume(), 0, 1)

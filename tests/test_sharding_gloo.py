@@ -150,3 +150,80 @@ def test_batched_problems_shard_by_rank():
         assert parts == bench.shard_problems(work, world)
         loads = [sum(work[p] for p in part) for part in parts]
         assert max(loads) - min(loads) <= max(work)
+
+
+class _OracleQuarterPlan(_OraclePlan):
+    """_OraclePlan with the quarter-set halves (recon_mlem_forward_quarters /
+    recon_mlem_backward_quarters): base views first .. first+count-1 of each of
+    the four quarters."""
+
+    quarter_sets = True
+
+    def _ranges(self, first, count):
+        q = self.nproj // 4
+        return [(first + r * q, count) for r in range(4)]
+
+    def mlem_forward_quarters(self, g, f, first, count):
+        self.ratios = []
+        for a, c in self._ranges(first, count):
+            self.mlem_forward(g, f, a, c)
+            self.ratios.append(self.ratio)
+
+    def mlem_backward_quarters(self, ht, first, count):
+        total = np.zeros(ht.numel())
+        for (a, c), ratio in zip(self._ranges(first, count), self.ratios):
+            total += self.bp(ratio, a, c)
+        ht.copy_(torch.from_numpy(total))
+
+
+def _quarter_worker(rank, world, init_file, out_dir):
+    dist.init_process_group("gloo", init_method=f"file://{init_file}", rank=rank, world_size=world)
+    from recon_b200.sharding import sharded_mlem_iteration
+
+    O, cfg, g, _ = _setup()
+    nproj, dang = 12, np.float32(30.0)
+    meas = np.random.default_rng(5).random(nproj * g.npix) * 2.0
+    P = _OracleQuarterPlan(O, g, nproj, dang)
+    f = torch.ones(g.nvox, dtype=torch.float64)
+    ht = torch.zeros(g.nvox, dtype=torch.float64)
+    for _ in range(2):
+        sharded_mlem_iteration(P, torch.from_numpy(meas), f, ht)
+    np.save(os.path.join(out_dir, f"q{rank}.npy"), f.numpy())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_mlem_quarter_sets_two_ranks():
+    """Plans whose back projection takes quarter sets are split by quarter sets
+    (rank 0: base views 0, 1 of each quarter; rank 1: base view 2); the result
+    is the single-process iteration's."""
+    out_dir = tempfile.mkdtemp()
+    init_file = os.path.join(out_dir, "init")
+    mp.start_processes(_quarter_worker, args=(2, init_file, out_dir), nprocs=2, start_method="spawn")
+    f0 = np.load(os.path.join(out_dir, "q0.npy"))
+    assert np.array_equal(f0, np.load(os.path.join(out_dir, "q1.npy")))
+    O, cfg, g, _ = _setup()
+    nproj, dang = 12, np.float32(30.0)
+    meas = np.random.default_rng(5).random(nproj * g.npix) * 2.0
+    fp, bp = _projector(O, g, nproj, dang)
+    sens = O.x_bp_all(g, nproj, dang, np.ones(nproj * g.npix), threads=1)
+    f = np.ones(g.nvox)
+    for _ in range(2):
+        hf = fp(f, 0, nproj)
+        ratio = np.where(hf != 0, meas / np.where(hf != 0, hf, 1), 0.0)
+        f = np.where(sens != 0, f * bp(ratio, 0, nproj) / np.where(sens != 0, sens, 1), 0.0)
+    assert np.max(np.abs(f - f0)) <= 1e-12 * np.max(np.abs(f))
+
+
+def test_quarter_sets_partition():
+    """The ranks' quarter sets cover every view exactly once."""
+    from recon_b200.sharding import view_range
+
+    for n in (4, 12, 360, 720):
+        for w in (1, 2, 3, 8):
+            q = n // 4
+            views = []
+            for r in range(w):
+                a, c = view_range(q, r, w)
+                views += [a + k + s * q for s in range(4) for k in range(c)]
+            assert sorted(views) == list(range(n))
