@@ -287,6 +287,7 @@ struct GatherView {
     float2 c[2];   // {ca, cb}
     int u_lo, u_hi;
     unsigned flags;
+    unsigned view;  // the view's index (fills the struct's 16-byte alignment)
 };
 
 // Column (i, j) of the volume, [Xa, Xb] x [Ya, Yb], seen from one view (see
@@ -311,6 +312,7 @@ __device__ __forceinline__ GatherView gather_view(const ExactGeom& G, const Gath
     }
     GatherView V;
     V.flags = 0u;
+    V.view = view;
     if (behind) {  // not for a volume in front of the source; stays exact anyway
         V.u_lo = 0;
         V.u_hi = G.Nu - 1;
@@ -971,7 +973,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 3) bp_gather_pairs_kernel(
 // sums in another order.
 // Dynamic shared memory: the rows' z planes (Nv float4), then the epilogue's
 // staging area [warp][d_r][lower voxels, mirrors][PS * 32].
-template <int EPI, class ST, int PS>
+template <int EPI, class ST, int PS, bool SET = false>
 __global__ void __launch_bounds__(kGatherWarps * 32, PS <= 2 ? 3 : 2) bp_gather_quarter_kernel(
     ExactGeom G, GatherConst C, const float4* __restrict__ txy, const int2* __restrict__ kxy,
     const float2* __restrict__ cs, const ZParam* __restrict__ zp, unsigned nview, unsigned m0, unsigned mc,
@@ -994,11 +996,11 @@ __global__ void __launch_bounds__(kGatherWarps * 32, PS <= 2 ? 3 : 2) bp_gather_
     const int i = i0 + warp % kGatherTileX, j = j0 + warp / kGatherTileX;
     const bool active = i < H && j < H;
     const unsigned Q = nview / 4u;
-    // the views summed: base views m0 .. m0 + mc - 1 of each quarter (all views
-    // for m0 = 0, mc = Q), item i being view m0 + i % mc + (i / mc) Q; the set is
-    // closed under quarter turns, so every turned column gets the same views
-    const unsigned nview_w = active ? 4u * mc : 0u;
-    auto view_of = [&](unsigned it) { return m0 + it % mc + (it / mc) * Q; };
+    // the views summed: all views (item i is view i), or with SET base views m0 ..
+    // m0 + mc - 1 of each quarter, item i being view m0 + i % mc + (i / mc) Q (the
+    // set is closed under quarter turns, so every turned column gets the same views)
+    const unsigned nview_w = active ? (SET ? 4u * mc : nview) : 0u;
+    auto view_of = [&](unsigned it) { return SET ? m0 + it % mc + (it / mc) * Q : it; };
     GatherView* sv = sview[warp];
     const float Xa = G.P0[0] + i * G.vox[0], Xb = Xa + G.vox[0];
     const float Ya = G.P0[1] + j * G.vox[1], Yb = Ya + G.vox[1];
@@ -1111,7 +1113,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32, PS <= 2 ? 3 : 2) bp_gather_
                                        dz32);
             __syncwarp();
             for (unsigned q = 0; q < nb; ++q) {
-                const unsigned m = view_of(vb + q);
+                const unsigned m = SET ? sv[q].view : vb + q;
                 const ST* vm[4];  // views m + rQ (mod N) from detector column 0
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
@@ -2035,7 +2037,7 @@ bool exact_quarter_sets(const Plan& P)
 }
 
 // vals: view 0 of the plan's views; m0, mc: the base views of the quarter set
-template <int EPI, class ST, int PS>
+template <int EPI, class ST, int PS, bool SET = false>
 static recon_status_t launch_gather_quarter(Plan& P, const ST* vals, size_t view_stride, float* vol,
                                             const float* sens, cudaStream_t s, unsigned long long* npairs,
                                             unsigned m0, unsigned mc)
@@ -2043,7 +2045,7 @@ static recon_status_t launch_gather_quarter(Plan& P, const ST* vals, size_t view
     const ExactGeom& E = P.eg;
     const exact::GatherConst C = gather_const(P, vol, sens);
     const size_t smem = quarter_dynamic_smem<PS>(P);
-    auto kernel = exact::bp_gather_quarter_kernel<EPI, ST, PS>;
+    auto kernel = exact::bp_gather_quarter_kernel<EPI, ST, PS, SET>;
     if (smem + kQuarterStaticSmem > 48 * 1024)
         RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     constexpr int tx = exact::kGatherTileX, ty = exact::kGatherWarps / exact::kGatherTileX;
@@ -2161,10 +2163,10 @@ recon_status_t exact_bp_quarters(Plan& P, unsigned first, unsigned count, float*
         using ST = decltype(tag);
         const ST* vals = static_cast<const ST*>(P.d_ratio);
         switch (gather_quarter_slots(P.eg.Z)) {
-            case 1: return launch_gather_quarter<0, ST, 1>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
-            case 2: return launch_gather_quarter<0, ST, 2>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
-            case 3: return launch_gather_quarter<0, ST, 3>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
-            default: return launch_gather_quarter<0, ST, 4>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+            case 1: return launch_gather_quarter<0, ST, 1, true>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+            case 2: return launch_gather_quarter<0, ST, 2, true>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+            case 3: return launch_gather_quarter<0, ST, 3, true>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
+            default: return launch_gather_quarter<0, ST, 4, true>(P, vals, qv, vol, nullptr, s, nullptr, first, count);
         }
     };
     if (P.opt.sino == RECON_SINO_BF16) return run(__nv_bfloat16{});
