@@ -865,6 +865,24 @@ def main():
         torch.cuda.synchronize()
         out["sensitivity_ms"] = s0.elapsed_time(s1)
         del sens
+        if P.quarter_sets:
+            # one rank's back projection when two ranks split the views: a quarter set
+            # (half the base views of each quarter) against a contiguous half range
+            def bp_ms(call):
+                call()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                call()
+                e1.record()
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1)
+
+            q = nviews // 4
+            P.mlem_forward(g, f)
+            out["two_rank_split_bp_ms"] = {
+                "quarter_set": bp_ms(lambda: P.mlem_backward_quarters(ht, 0, q // 2)),
+                "contiguous_range": bp_ms(lambda: P.mlem_backward(ht, 0, 4 * (q // 2))),
+                "views_per_rank": 4 * (q // 2)}
     out["e2e"] = e2e
     out["clocks"] = clk
     if world == 1:
