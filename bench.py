@@ -68,15 +68,34 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+    """SM clock and throttle-reason samples while the timed region runs: read
+    through NVML every 10 ms (a timed region of ~0.1 s gives about ten), or
+    from nvidia-smi every 200 ms where NVML cannot be loaded.  Reads only."""
 
     FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
               "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
               "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.lines: list[str] = []
+        self.samples: list[tuple[float, float, int]] = []  # NVML: (sm MHz, max sm MHz, reason bits)
         self.proc = None
+        self.nvml = None
+        self.done = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.bits = [getattr(pynvml, "nvmlClocksEventReason" + n) for n in
+                         ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(index), "--query-gpu=" + ",".join(self.FIELDS),
@@ -87,36 +106,57 @@ class ClockSampler:
         except (OSError, FileNotFoundError):
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml, self.handle
+        while not self.done.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), int(rs)))
+            except Exception:
+                return
+            self.done.wait(0.01)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self) -> dict | None:
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < len(self.FIELDS):
-                continue
+        if self.nvml is not None:
+            self.done.set()
+            self.t.join(timeout=5)
+            for a, b, rs in self.samples:
+                sm.append(a)
+                mx.append(b)
+                reasons.update(nm for nm, bit in zip(self.NAMES, self.bits) if rs & bit)
+            source = "nvml, 10 ms"
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[4:8]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            for ln in self.lines:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < len(self.FIELDS):
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    mx.append(float(parts[1]))
+                except ValueError:
+                    continue
+                for nm, val in zip(self.NAMES, parts[4:8]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+            source = "nvidia-smi, 200 ms"
+        else:
+            return None
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": source}
 
 
 def gpu_index(local_rank: int) -> int:
